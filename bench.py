@@ -1,0 +1,414 @@
+#!/usr/bin/env python
+"""Benchmark: hex8 assemble + PCG + compliance gradient, mixed precision vs plain FP64, on B200.
+
+One step = the whole hot path over one synthetic cantilever (default 128x32x32 hex8, 2.0 x 0.4 x
+0.4 m, E = 210 GPa, nu = 0.3, x = 0 clamped, random N(0,1)*1e6 Pa per-node tip traction):
+node topology + CSR pattern + element matrices + CSR values (FP64 + FP32 copy + Jacobi
+diagonal) + Jacobi-PCG to the residual tolerance + SIMP compliance gradient dC/drho_e (p = 3,
+rho = 1, rho_min = 1e-9).  Inputs are resident in HBM when the timed region starts; K_ff
+(> 400 MB FP64) is larger than the 126 MB L2, so no explicit L2 flush is done between steps.
+
+`value` is the mixed-precision step time (ms, lower is better); the plain FP64 step time is
+reported beside it.  `e2e` is the same step through the public FESystem API from host numpy
+arrays, host<->device copies included.  With --gpus N (torchrun) every rank runs an
+independent replica of the workload (the path has no cross-GPU exchange) and the slowest
+rank's time is reported.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "computation-suite_b200"))
+
+import numpy as np  # noqa: E402
+
+METRIC = "hex8 assemble+PCG+grad time at rel err 1e-8, mixed vs plain FP64, 1 B200"
+PENAL, RHO_MIN = 3.0, 1e-9
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--shape", type=int, nargs=3, default=(128, 32, 32))
+    ap.add_argument("--tol", type=float, default=1e-9)
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations timed for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--spmv-reps", type=int, default=20)
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------- distributed
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+        torch.cuda.set_device(local)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=600),
+                                             device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def barrier(world):
+    import torch
+    if world > 1:
+        torch.distributed.barrier()
+
+
+def max_over_ranks(v, world):
+    import torch
+    if world == 1:
+        return v
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------- clocks
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.proc = None
+        self.path = None
+        self.gpu = gpu_index
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                                          "-lms", "200", "-i", str(self.gpu)], stdout=self.out,
+                                         stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if v.lower().startswith("active")})
+        loaded = [s for s in sm if mx and s > 0.5 * max(mx)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ----------------------------------------------------------------------------- workload
+def build_workload(shape):
+    from feab200 import cantilever
+    return cantilever.random_tip_cantilever(*shape)
+
+
+class DeviceProblem:
+    """Inputs resident in HBM: coordinates, connectivity, reduced load vector, densities."""
+
+    def __init__(self, c, device):
+        import torch
+        self.c = c
+        self.device = device
+        self.coords = torch.as_tensor(c.mesh.nodes).to(device)
+        self.conn = torch.as_tensor(c.mesh.elements.astype(np.int32)).to(device)
+        self.fixed = c.fixed
+        self.free = torch.as_tensor(c.free).to(device)
+        self.Ff = torch.as_tensor(c.F[c.free]).to(device)
+        self.rho = torch.ones(len(c.mesh.elements), dtype=torch.float64, device=device)
+        self.n_dof = c.n_dof
+
+    def step(self, precision, tol):
+        import torch
+        from feab200.device import DeviceMesh, pcg_solve
+        dm = DeviceMesh(self.coords, self.conn, device=self.device)
+        pat = dm.pattern(self.fixed)
+        ke = dm.element_stiffness(self.c.D)
+        op = dm.assemble(ke, pat, want32=(precision == "fp32"))
+        x, info = pcg_solve(op, self.Ff, tol=tol, precision=precision)
+        if info.status != 0:
+            raise RuntimeError(f"PCG failed: {info}")
+        u = torch.zeros(self.n_dof, dtype=torch.float64, device=self.device)
+        u[self.free] = x
+        dc = dm.simp_vjp(self.c.D, self.rho, PENAL, RHO_MIN, u)
+        return x, dc, info, op
+
+
+def time_steps(prob, precision, tol, steps, warmup, world):
+    import torch
+    from feab200 import _lib as L
+    for _ in range(warmup):
+        prob.step(precision, tol)
+    torch.cuda.synchronize()
+    barrier(world)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = L.lib.feab_launch_count()
+    start.record()
+    for _ in range(steps):
+        x, dc, info, op = prob.step(precision, tol)
+    end.record()
+    torch.cuda.synchronize()
+    launches = int(L.lib.feab_launch_count() - n0)
+    ms = start.elapsed_time(end) / steps
+    return max_over_ranks(ms, world), x, dc, info, op, launches
+
+
+def e2e_steps(c, precision, tol, steps, warmup):
+    """The step through the public API from host numpy arrays (copies inside the timed region)."""
+    import torch
+    import feab200
+    from feab200 import topopt
+
+    def one():
+        mesh = feab200.Mesh(nodes=c.mesh.nodes, elements=c.mesh.elements)
+        fs = feab200.FESystem(mesh, feab200.Hex8Solid3D(), sparse=True, device="cuda")
+        fs.assemble_stiffness(c.D)
+        fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+        fs.F[:] = c.F
+        U = fs.solve_static(method="pcg", tol=tol, precision=precision)
+        ke_unit, conn = topopt.unit_stiffness_stack(fs, c.D)
+        dc = topopt.compliance_sensitivity_closed_form(ke_unit, conn, 3, np.asarray(U),
+                                                       np.ones(len(c.mesh.elements)), PENAL, RHO_MIN)
+        return U, dc
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        U, dc = one()
+    torch.cuda.synchronize()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    N, E, n = len(c.mesh.nodes), len(c.mesh.elements), len(c.free)
+    h2d = N * 3 * 8 + E * 8 * 4 + n * 8 + 3 * N * 8 + E * 8     # nodes, conn, F_free, U (for dC/drho), rho
+    d2h = 3 * N * 8 + E * 8                                      # U, dC/drho
+    return ms, h2d, d2h
+
+
+def spmv_bytes(op, precision):
+    """Algorithmic bytes of one launch of the PCG's SpMV kernel for `precision`, counted from
+    what the kernel must read and write once: values, column indices (one row per node
+    group, since the rows of a node share them), row/group pointers, the x vector and y."""
+    p = op.pattern
+    rp = p.row_ptr.cpu().numpy().astype(np.int64)
+    gp = p.group_ptr.cpu().numpy().astype(np.int64)
+    f = np.diff(gp)
+    lens = rp[gp[:-1] + 1] - rp[gp[:-1]]
+    lead = int(lens.sum())
+    n, nnz, G = p.n, p.nnz, p.n_groups
+    ptrs = 4 * (n + 1) + 4 * (G + 1)
+    if precision == "fp64":
+        return nnz * 8 + 4 * lead + ptrs + 2 * n * 8
+    if precision == "fp32":
+        return nnz * 4 + 4 * lead + ptrs + 2 * n * 4
+    own = int((f * f).sum())                                   # own-node block entries are skipped
+    return (nnz - own) * 6 + 4 * lead + ptrs + G + 24 * n + 2 * n * 8
+
+
+def spmv_roofline(op, precision, reps, peak_gbs):
+    """Average duration of the PCG's SpMV kernel with CUDA events on the launching stream;
+    L2 is flushed before each launch by a 256 MB write."""
+    import torch
+    from feab200.device import spmv
+    dev = op.vals64.device
+    dt = torch.float32 if precision == "fp32" else torch.float64
+    x = torch.randn(op.n, dtype=dt, device=dev)
+    y = torch.empty(op.n, dtype=dt, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    spmv(op, x, precision, out=y)
+    times = []
+    for _ in range(reps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        spmv(op, x, precision, out=y)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) * 1e-3)
+    t = statistics.mean(times)
+    nbytes = spmv_bytes(op, precision)
+    p = op.pattern
+    bytes_csr = p.nnz * ((4 if precision == "fp32" else 8) + 4) + 4 * (p.n + 1) + 2 * p.n * (4 if precision == "fp32" else 8)
+    achieved = nbytes / t / 1e9
+    kern = {"fp64": "k_spmv<double>", "fp32": "k_spmv<float>", "mixed": "k_spmv_diff"}[precision]
+    return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak_gbs, "unit": "GB/s",
+            "frac": round(achieved / peak_gbs, 3), "traffic": None,
+            "kernel": f"{kern} (the SpMV of PCG step A, {precision})", "bytes_per_launch": int(nbytes),
+            "csr_formula_bytes": int(bytes_csr), "launch_us": round(t * 1e6, 2)}
+
+
+def measured_peak():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+# ----------------------------------------------------------------------------- CPU (oracle)
+class CpuReference:
+    """The oracle (NumPy/SciPy restatement of the reference path) on the host cores: the full
+    assembly once, then bounded samples of PCG iterations, extrapolated to a full solve."""
+
+    def __init__(self, c):
+        import oracle as O
+        self.O, self.c = O, c
+        X, el = c.mesh.nodes, c.mesh.elements
+        t0 = time.perf_counter()
+        self.ke = O.hex8_element_stiffness(X[el], c.D)
+        K = O.structural_csr(self.ke, el, c.n_dof)
+        self.Kff = O.reduce_free(K, c.free)
+        self.dinv = O.jacobi_inverse_diagonal(self.Kff)
+        self.t_asm = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        O.compliance_sensitivity_closed_form(self.ke, el, np.zeros(c.n_dof), np.ones(len(el)), PENAL, RHO_MIN)
+        self.t_grad = time.perf_counter() - t0
+
+    def iteration_time(self, iters):
+        b = self.c.F[self.c.free]
+        t0 = time.perf_counter()
+        try:
+            self.O.preconditioned_cg(self.Kff, b, self.dinv, tol=1e-300, maxiter=iters)
+        except RuntimeError:
+            pass
+        return (time.perf_counter() - t0) / iters
+
+    def step_ms(self, iters_full, iters_sample):
+        return (self.t_asm + self.iteration_time(iters_sample) * iters_full + self.t_grad) * 1e3
+
+    def describe(self, iters_full, iters_sample, value):
+        return {"value": round(value, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+                "sample": (f"oracle on {os.cpu_count()} host threads (SciPy CSR SpMV single-threaded): full assembly "
+                           f"{self.t_asm:.2f} s + {iters_sample} timed PCG iterations extrapolated to "
+                           f"{iters_full} + dC/drho {self.t_grad:.2f} s")}
+
+
+def gpu_index(local):
+    vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+    ids = [v for v in vis.split(",") if v.strip()]
+    if ids and local < len(ids) and ids[local].strip().isdigit():
+        return int(ids[local])
+    return local
+
+
+# ----------------------------------------------------------------------------- main
+def main():
+    args = parse()
+    import torch
+    world, rank, local = dist_setup(args.gpus)
+    shape = tuple(args.shape)
+    workload = (f"cantilever hex8 {shape[0]}x{shape[1]}x{shape[2]} (2.0x0.4x0.4 m, random tip traction, "
+                f"x=0 clamped): topology+pattern+Ke+CSR assembly + Jacobi-PCG (rel residual {args.tol:g}) "
+                f"+ SIMP dC/drho")
+    c = build_workload(shape)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        # Iterations the reference recurrence needs on this workload at tol 1e-9: 1267, counted by
+        # running the oracle's preconditioned_cg to convergence on the host (the GPU FP64 solve
+        # takes the same 1267); used to extrapolate the bounded CPU samples
+        iters = int(os.environ.get("FEAB_REF_ITERS", "0")) or (1267 if shape == (128, 32, 32) else 10 * len(c.free))
+        ref = CpuReference(c)
+        for _ in range(args.warmup):
+            ref.iteration_time(1)
+        vals = [ref.step_ms(iters, args.cpu_iters) for _ in range(args.steps)]
+        v = statistics.mean(vals)
+        print(json.dumps({"impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": "ms",
+                          "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 1),
+                          "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                          "data": "synthetic", "config": {"workload": workload, "parallelism": "replicas"},
+                          "cpu_baseline": ref.describe(iters, args.cpu_iters, v),
+                          "e2e": {"value": round(v, 1), "unit": "ms", "h2d_bytes_per_step": 0,
+                                  "d2h_bytes_per_step": 0}}), flush=True)
+        return
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    prob = DeviceProblem(c, dev)
+    clocks = ClockSampler(gpu_index(local))
+    # plain FP64 first, then mixed (the headline)
+    ms64, x64, dc64, info64, op64, _ = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
+    clocks.start()
+    ms32, x32, dc32, info32, op, launches = time_steps(prob, "mixed", args.tol, args.steps, args.warmup, world)
+    clk = clocks.stop()
+    # the FP32-everything variant, one solve, for reference
+    t0 = time.perf_counter()
+    xf, _, infof, _ = prob.step("fp32", args.tol)
+    torch.cuda.synchronize()
+    msf = (time.perf_counter() - t0) * 1e3
+    # accuracy: against a tight FP64 solve of the same system
+    from feab200.device import pcg_solve
+    xt, infot = pcg_solve(op64, prob.Ff, tol=1e-13, precision="fp64")
+    rel = lambda a: float(torch.linalg.norm(a - xt) / torch.linalg.norm(xt))  # noqa: E731
+    err32, err64, errf = rel(x32), rel(x64), rel(xf)
+    dc_err = float(torch.linalg.norm(dc32 - dc64) / torch.linalg.norm(dc64))
+    peak, peak_kind = measured_peak()
+    roof = spmv_roofline(op, "mixed", args.spmv_reps, peak)
+    roof64 = spmv_roofline(op64, "fp64", args.spmv_reps, peak)
+    for r in (roof, roof64):
+        r["peak_source"] = f"MEASURED_PEAKS.json hbm_gbs (of {peak_kind})"
+    e2e_ms, h2d, d2h = e2e_steps(c, "mixed", args.tol, args.e2e_steps, 1)
+    e2e_ms = max_over_ranks(e2e_ms, world)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        ref = CpuReference(c)
+        cpu = ref.describe(info64.iters, args.cpu_iters, ref.step_ms(info64.iters, args.cpu_iters))
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": round(ms32, 3), "unit": "ms", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(ms32, 3), "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": workload, "n_free": op.n, "nnz": op.nnz, "tol": args.tol,
+                       "precision": ("mixed: SpMV on 48-bit (36-bit mantissa) values in difference form, FP64 vectors "
+                          "and scalars, FP64 reliable residual replacement"),
+                       "l2": "inputs larger than L2 (K_ff FP64 values alone exceed 126 MB); no flush",
+                       "parallelism": f"replicas x{world}"},
+            "plain_fp64_ms": round(ms64, 3), "mixed_speedup_vs_fp64": round(ms64 / ms32, 3),
+            "fp32_everything_ms": round(msf, 3),
+            "iters": {"mixed": info32.iters, "fp64": info64.iters, "fp32": infof.iters,
+                      "reliable_updates": info32.reliable_updates},
+            "rel_err": {"mixed_vs_fp64_tight": err32, "fp64_vs_fp64_tight": err64, "fp32_vs_fp64_tight": errf,
+                        "dc_mixed_vs_fp64": dc_err, "tight_tol": 1e-13, "mixed_relres_fp64": info32.relres},
+            "roofline": roof,
+            "roofline_fp64": roof64,
+            "cpu_baseline": cpu,
+            "e2e": {"value": round(e2e_ms, 2), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "path": "FESystem + topopt from host numpy (pageable) arrays"},
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,907 @@
+// Jacobi-preconditioned conjugate gradients on the GPU (d).
+//
+// One CG iteration is one "step" of two kernels:
+//   A  p_new = z + beta p_old (formed on the fly inside the SpMV gathers, written for the
+//      warp's own rows into the other half of a p ping-pong buffer), Ap = K p_new, p_new.Ap
+//   B  x += alpha p, r -= alpha Ap, z = M r, r.r and r.z, convergence test, beta
+// The p update is therefore never a separate pass, and its arithmetic is exactly the
+// reference's p = z + beta p.  Scalars live in a device PcgState; each kernel's last block
+// (ticket counter) reduces the per-block partials in a fixed order, so results are
+// bit-reproducible.  A chunk of steps is captured once in a CUDA graph and replayed; kernels
+// return at once when the state says done, and the host polls the done flag one chunk
+// behind, so there is no host sync per iteration.
+//
+// SpMV: one warp per row group (the rows of one mesh node share their column list), all
+// columns of a group (<= 96 per pass) issued before any is consumed, so each warp keeps a
+// whole group's index, value and gather loads in flight.
+//
+// Precisions (feab_pcg_params.precision):
+//   FEAB_PREC_FP64   the reference recurrence (iterative_solvers.py:434-481) in FP64.
+//   FEAB_PREC_MIXED  FP64 vectors and scalars; the SpMV reads 6-byte values (doubles rounded
+//                    to 36 mantissa bits) and applies K in difference form,
+//                    y_a = sum_{b != a} K_ab (x_b - x_a) + S_a x_a, S_a = sum_b K_ab exact in FP64,
+//                    so value rounding multiplies x_b - x_a (small for the smooth low modes)
+//                    instead of x.  The residual is replaced by the FP64 b - K x (FP64 SpMV)
+//                    whenever it has dropped by reliable_delta, and convergence is declared on
+//                    that FP64 residual only.
+//   FEAB_PREC_FP32   FP32 values, FP32 p/r/Ap/x-correction, FP64 scalars, FP64 reliable updates
+//                    folding the correction into an FP64 solution.
+#include <algorithm>
+#include <cmath>
+#include "feab_common.cuh"
+
+namespace feab {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kModeCG = 0;
+constexpr int kModeReliable = 1;
+
+struct PcgState {
+  double bnorm, tol, delta;
+  double rz_old, pAp, alpha, beta, rr, relres, rmax, rr64;
+  int32_t iters, maxiter, done, status;
+  int32_t mode, p_pending, psel, xsel, reliable_updates;
+  uint32_t ticket[4];
+};
+
+struct PcgArgs {
+  int32_t n, n_groups;
+  const int32_t* row_ptr;
+  const int32_t* col_idx;
+  const int32_t* group_ptr;
+  const double* vals64;
+  const float* vals32;
+  // difference-form operator (mixed)
+  const uint32_t* vhi;
+  const uint16_t* vlo;
+  const int32_t* tcol;     // column | (DOF component << 30)
+  const uint8_t* gmask;    // free-DOF mask of each group's node
+  const double* S;         // n x 3 row-block sums
+  const double* dinv64;
+  const float* dinv32;
+  const double* b;
+  const double* x0;
+  double* x;
+  PcgState* S_;
+  double* partials;
+  double *r, *z, *p0, *p1, *Ap;      // FP64 vectors (fp64, mixed)
+  double *x64a, *x64b, *r64;         // fp32 mode: FP64 solution ping-pong + FP64 residual
+  float *r32, *z32, *q0, *q1, *Ap32, *x32;  // fp32 mode vectors (q = p)
+  int use_dinv;
+};
+
+__device__ __forceinline__ bool last_block_of(uint32_t* ticket) {
+  __shared__ bool is_last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    const uint32_t t = atomicAdd(ticket, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  return is_last;
+}
+
+// Writes this block's NV partial sums; the last block reduces all blocks' partials in a fixed
+// order into tot[] and returns true.
+template <int NV>
+__device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, uint32_t* ticket, double (&tot)[NV]) {
+  __shared__ double sh[NV * 32];
+  block_sum<NV>(v, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) partials[k * gridDim.x + blockIdx.x] = v[k];
+  }
+  if (!last_block_of(ticket)) return false;
+  double s[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) s[k] = 0.0;
+  for (int i = threadIdx.x; i < (int)gridDim.x; i += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) s[k] += __ldcg(&partials[k * gridDim.x + i]);
+  }
+  block_sum<NV>(s, sh);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int k = 0; k < NV; ++k) tot[k] = s[k];
+    *ticket = 0;
+  }
+  return true;
+}
+
+__device__ __forceinline__ void group_rows(const PcgArgs& A, int g, int& r0, int& f) {
+  if (A.group_ptr) {
+    r0 = A.group_ptr[g];
+    f = A.group_ptr[g + 1] - r0;
+  } else {
+    r0 = g;
+    f = 1;
+  }
+}
+
+// acc[k] = sum_c vals[row r0+k, c] * xf(col c) for the f (<= 3) rows of a group.
+template <typename AT, typename VT, typename XF>
+__device__ __forceinline__ void group_spmv(const PcgArgs& A, const VT* __restrict__ vals, int r0, int f, int lane,
+                                           XF xf, AT (&acc)[3]) {
+  const int s0 = A.row_ptr[r0];
+  const int len = A.row_ptr[r0 + 1] - s0;
+  const int32_t* __restrict__ col = A.col_idx + s0;
+  const VT* __restrict__ v0 = vals + s0;
+  AT a0 = 0, a1 = 0, a2 = 0;
+  for (int c = lane; c < len; c += 96) {
+    const bool p1 = c + 32 < len, p2 = c + 64 < len;
+    const int j0 = __ldg(col + c);
+    const int j1 = p1 ? __ldg(col + c + 32) : 0;
+    const int j2 = p2 ? __ldg(col + c + 64) : 0;
+    const AT w00 = (AT)__ldg(v0 + c);
+    const AT w01 = p1 ? (AT)__ldg(v0 + c + 32) : AT(0);
+    const AT w02 = p2 ? (AT)__ldg(v0 + c + 64) : AT(0);
+    AT w10 = 0, w11 = 0, w12 = 0, w20 = 0, w21 = 0, w22 = 0;
+    if (f > 1) {
+      w10 = (AT)__ldg(v0 + len + c);
+      w11 = p1 ? (AT)__ldg(v0 + len + c + 32) : AT(0);
+      w12 = p2 ? (AT)__ldg(v0 + len + c + 64) : AT(0);
+    }
+    if (f > 2) {
+      w20 = (AT)__ldg(v0 + 2 * len + c);
+      w21 = p1 ? (AT)__ldg(v0 + 2 * len + c + 32) : AT(0);
+      w22 = p2 ? (AT)__ldg(v0 + 2 * len + c + 64) : AT(0);
+    }
+    const AT x0 = xf(j0);
+    const AT x1 = p1 ? xf(j1) : AT(0);
+    const AT x2 = p2 ? xf(j2) : AT(0);
+    a0 += w00 * x0 + w01 * x1 + w02 * x2;
+    a1 += w10 * x0 + w11 * x1 + w12 * x2;
+    a2 += w20 * x0 + w21 * x1 + w22 * x2;
+  }
+  acc[0] = warp_sum(a0);
+  acc[1] = f > 1 ? warp_sum(a1) : AT(0);
+  acc[2] = f > 2 ? warp_sum(a2) : AT(0);
+}
+
+__device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
+}
+
+// Difference-form SpMV over one group with 48-bit values:
+// acc[k] = sum_{c, col(c) not in own node} v[c] (x(col c) - xs[j(c)]) + sum_j S[r0+k][j] xs[j].
+template <typename XF>
+__device__ __forceinline__ void group_spmv_diff(const PcgArgs& A, int g, int r0, int f, int lane, XF xf,
+                                                double (&acc)[3]) {
+  const int mask = A.gmask[g];
+  double xs[3];
+#pragma unroll
+  for (int j = 0; j < 3; ++j) xs[j] = ((mask >> j) & 1) ? xf(r0 + __popc(mask & ((1 << j) - 1))) : 0.0;
+  const int s0 = A.row_ptr[r0];
+  const int len = A.row_ptr[r0 + 1] - s0;
+  const int32_t* __restrict__ col = A.tcol + s0;
+  double a[3] = {0.0, 0.0, 0.0};
+  for (int c0 = lane; c0 < len; c0 += 96) {
+    int jj[3];
+    double d[3];
+#pragma unroll
+    for (int u = 0; u < 3; ++u) {
+      const int c = c0 + 32 * u;
+      const unsigned t = c < len ? (unsigned)__ldg(col + c) : 0u;
+      const int cj = (int)(t & 0x3fffffffu);
+      const bool own = c >= len || (cj >= r0 && cj < r0 + f);
+      jj[u] = own ? -1 : c;
+      d[u] = own ? 0.0 : xf(cj) - xs[t >> 30];
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k < f) {
+        const int off = s0 + k * len;
+#pragma unroll
+        for (int u = 0; u < 3; ++u)
+          if (jj[u] >= 0) a[k] += dec48(__ldg(A.vhi + off + jj[u]), __ldg(A.vlo + off + jj[u])) * d[u];
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    acc[k] = k < f ? warp_sum(a[k]) : 0.0;
+    if (k < f) acc[k] += A.S[(r0 + k) * 3 + 0] * xs[0] + A.S[(r0 + k) * 3 + 1] * xs[1] + A.S[(r0 + k) * 3 + 2] * xs[2];
+  }
+}
+
+__device__ __forceinline__ double pick3(const double (&a)[3], int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
+__device__ __forceinline__ float pick3(const float (&a)[3], int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
+
+__global__ void k_init_state(PcgState* S, double tol, double delta, int maxiter) {
+  S->bnorm = 1.0;
+  S->tol = tol;
+  S->delta = delta;
+  S->rz_old = S->pAp = S->alpha = S->beta = S->rr = S->relres = S->rmax = S->rr64 = 0.0;
+  S->iters = 0;
+  S->maxiter = maxiter;
+  S->done = 0;
+  S->status = FEAB_OK;
+  S->mode = kModeCG;
+  S->p_pending = 0;
+  S->psel = 0;
+  S->xsel = 0;
+  S->reliable_updates = 0;
+  for (int k = 0; k < 4; ++k) S->ticket[k] = 0;
+}
+
+// r = b - K64 x0 (plain form, FP64); ||b||, ||r||; early exit as iterative_solvers.py:437-443.
+// fp32 mode writes the FP64 residual to r64, the others to r.
+template <int PREC>
+__global__ void __launch_bounds__(kThreads) k_setup_a(PcgArgs A) {
+  PcgState* S = A.S_;
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int G = A.group_ptr ? A.n_groups : A.n;
+  double* r = PREC == FEAB_PREC_FP32 ? A.r64 : A.r;
+  double part[2] = {0.0, 0.0};
+  for (int g = wg; g < G; g += nw) {
+    int r0, f;
+    group_rows(A, g, r0, f);
+    double acc[3] = {0.0, 0.0, 0.0};
+    if (A.x0) group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.x0 + j); }, acc);
+    if (lane < f) {
+      const double bi = A.b[r0 + lane];
+      const double ri = bi - pick3(acc, lane);
+      r[r0 + lane] = ri;
+      part[0] += bi * bi;
+      part[1] += ri * ri;
+    }
+  }
+  double tot[2];
+  if (grid_reduce<2>(part, A.partials, &S->ticket[0], tot) && threadIdx.x == 0) {
+    double bn = sqrt(tot[0]);
+    if (bn == 0.0) bn = 1.0;
+    S->bnorm = bn;
+    S->rr = tot[1];
+    S->rr64 = tot[1];
+    S->relres = sqrt(tot[1]) / bn;
+    if (S->relres < S->tol) {
+      S->done = 1;
+      S->status = FEAB_OK;
+    }
+  }
+}
+
+// z = M r, p = z, rz = r.z (fp32 mode: r32 = (float) r64 first, x32 = 0).
+template <int PREC>
+__global__ void __launch_bounds__(kThreads) k_setup_b(PcgArgs A) {
+  PcgState* S = A.S_;
+  if (S->done) return;
+  double part[1] = {0.0};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x) {
+    if (PREC == FEAB_PREC_FP32) {
+      const float ri = (float)A.r64[i];
+      const float zi = A.use_dinv ? A.dinv32[i] * ri : ri;
+      A.r32[i] = ri;
+      A.z32[i] = zi;
+      A.q0[i] = zi;
+      A.x32[i] = 0.0f;
+      part[0] += (double)ri * (double)zi;
+    } else {
+      const double ri = A.r[i];
+      const double zi = A.use_dinv ? A.dinv64[i] * ri : ri;
+      A.z[i] = zi;
+      A.p0[i] = zi;
+      part[0] += ri * zi;
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.partials, &S->ticket[1], tot) && threadIdx.x == 0) {
+    S->rz_old = tot[0];
+    S->rmax = sqrt(S->rr);
+    S->mode = kModeCG;
+    S->p_pending = 0;
+    S->psel = 0;
+  }
+}
+
+// Step kernel A.
+template <int PREC>
+__global__ void __launch_bounds__(kThreads) k_step_a(PcgArgs A) {
+  PcgState* S = A.S_;
+  if (S->done) return;
+  const int mode = S->mode;
+  const int pend = S->p_pending;
+  const int psel = S->psel;
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int G = A.group_ptr ? A.n_groups : A.n;
+  double part[1] = {0.0};
+  if (PREC == FEAB_PREC_FP32 && mode == kModeReliable) {
+    // r64 = b - K64 (x64 + x32); x64' = x64 + x32 (other half of the ping-pong)
+    const double* xin = S->xsel ? A.x64b : A.x64a;
+    double* xout = S->xsel ? A.x64a : A.x64b;
+    for (int g = wg; g < G; g += nw) {
+      int r0, f;
+      group_rows(A, g, r0, f);
+      double acc[3];
+      group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(xin + j) + (double)__ldg(A.x32 + j); },
+                         acc);
+      if (lane < f) {
+        const int i = r0 + lane;
+        const double ri = A.b[i] - pick3(acc, lane);
+        A.r64[i] = ri;
+        xout[i] = xin[i] + (double)A.x32[i];
+        part[0] += ri * ri;
+      }
+    }
+  } else if (PREC == FEAB_PREC_MIXED && mode == kModeReliable) {
+    // FP64 residual with the exact FP64 values: r = b - K64 x
+    for (int g = wg; g < G; g += nw) {
+      int r0, f;
+      group_rows(A, g, r0, f);
+      double acc[3];
+      group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.x + j); }, acc);
+      if (lane < f) {
+        const int i = r0 + lane;
+        const double ri = A.b[i] - pick3(acc, lane);
+        A.r[i] = ri;
+        part[0] += ri * ri;
+      }
+    }
+  } else if (PREC == FEAB_PREC_FP32) {
+    const float beta = (float)S->beta;
+    const float* __restrict__ qo = psel ? A.q1 : A.q0;
+    float* __restrict__ qn = psel ? A.q0 : A.q1;
+    for (int g = wg; g < G; g += nw) {
+      int r0, f;
+      group_rows(A, g, r0, f);
+      float acc[3];
+      if (pend) {
+        group_spmv<float>(A, A.vals32, r0, f, lane,
+                          [&](int j) { return fmaf(beta, __ldg(qo + j), __ldg(A.z32 + j)); }, acc);
+      } else {
+        group_spmv<float>(A, A.vals32, r0, f, lane, [&](int j) { return __ldg(qo + j); }, acc);
+      }
+      if (lane < f) {
+        const int i = r0 + lane;
+        const float pi = pend ? fmaf(beta, qo[i], A.z32[i]) : qo[i];
+        if (pend) qn[i] = pi;
+        const float v = pick3(acc, lane);
+        A.Ap32[i] = v;
+        part[0] += (double)pi * (double)v;
+      }
+    }
+  } else {
+    const double beta = S->beta;
+    const double* __restrict__ po = psel ? A.p1 : A.p0;
+    double* __restrict__ pn = psel ? A.p0 : A.p1;
+    for (int g = wg; g < G; g += nw) {
+      int r0, f;
+      group_rows(A, g, r0, f);
+      double acc[3];
+      if (PREC == FEAB_PREC_MIXED) {
+        if (pend)
+          group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc);
+        else
+          group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(po + j); }, acc);
+      } else {
+        if (pend)
+          group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); },
+                             acc);
+        else
+          group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(po + j); }, acc);
+      }
+      if (lane < f) {
+        const int i = r0 + lane;
+        const double pi = pend ? A.z[i] + beta * po[i] : po[i];
+        if (pend) pn[i] = pi;
+        const double v = pick3(acc, lane);
+        A.Ap[i] = v;
+        part[0] += pi * v;
+      }
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.partials, &S->ticket[0], tot) && threadIdx.x == 0) {
+    if (mode == kModeReliable && PREC != FEAB_PREC_FP64) {
+      S->rr64 = tot[0];
+    } else {
+      if (pend) S->psel = psel ^ 1;
+      S->p_pending = 0;
+      S->pAp = tot[0];
+      if (!(tot[0] > 0.0)) {  // p^T A p <= 0: A is not SPD (iterative_solvers.py:450-454)
+        S->status = FEAB_NOT_SPD;
+        S->done = 1;
+      } else {
+        S->alpha = S->rz_old / tot[0];
+      }
+    }
+  }
+}
+
+// Step kernel B.
+template <int PREC>
+__global__ void __launch_bounds__(kThreads) k_step_b(PcgArgs A) {
+  PcgState* S = A.S_;
+  if (S->done) return;
+  const int mode = S->mode;
+  const int psel = S->psel;
+  const int stride = gridDim.x * blockDim.x;
+  double part[2] = {0.0, 0.0};
+  if (mode == kModeReliable && PREC == FEAB_PREC_FP32) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+      const float ri = (float)A.r64[i];
+      const float zi = A.use_dinv ? A.dinv32[i] * ri : ri;
+      A.r32[i] = ri;
+      A.z32[i] = zi;
+      A.x32[i] = 0.0f;
+      part[1] += (double)ri * (double)zi;
+    }
+  } else if (mode == kModeReliable && PREC == FEAB_PREC_MIXED) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+      const double ri = A.r[i];
+      const double zi = A.use_dinv ? A.dinv64[i] * ri : ri;
+      A.z[i] = zi;
+      part[1] += ri * zi;
+    }
+  } else if (PREC == FEAB_PREC_FP32) {
+    const float alpha = (float)S->alpha;
+    const float* __restrict__ q = psel ? A.q1 : A.q0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+      A.x32[i] = fmaf(alpha, q[i], A.x32[i]);
+      const float ri = fmaf(-alpha, A.Ap32[i], A.r32[i]);
+      A.r32[i] = ri;
+      const float zi = A.use_dinv ? A.dinv32[i] * ri : ri;
+      A.z32[i] = zi;
+      part[0] += (double)ri * (double)ri;
+      part[1] += (double)ri * (double)zi;
+    }
+  } else {
+    const double alpha = S->alpha;
+    const double* __restrict__ p = psel ? A.p1 : A.p0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+      A.x[i] += alpha * p[i];
+      const double ri = A.r[i] - alpha * A.Ap[i];
+      A.r[i] = ri;
+      const double zi = A.use_dinv ? A.dinv64[i] * ri : ri;
+      A.z[i] = zi;
+      part[0] += ri * ri;
+      part[1] += ri * zi;
+    }
+  }
+  double tot[2];
+  if (!grid_reduce<2>(part, A.partials, &S->ticket[1], tot) || threadIdx.x != 0) return;
+  if (mode == kModeCG) {
+    S->iters += 1;
+    S->rr = tot[0];
+    const double rel = sqrt(tot[0]) / S->bnorm;
+    if (PREC == FEAB_PREC_FP64) {
+      S->relres = rel;
+      if (rel < S->tol) {
+        S->done = 1;
+        S->status = FEAB_OK;
+        return;
+      }
+      if (S->iters >= S->maxiter || !(rel == rel)) {
+        S->done = 1;
+        S->status = FEAB_NOT_CONVERGED;
+        return;
+      }
+    } else if (rel < S->tol || sqrt(tot[0]) < S->delta * S->rmax || S->iters >= S->maxiter || !(rel == rel)) {
+      S->mode = kModeReliable;  // the next step replaces r by the FP64 residual; p waits for it
+      return;
+    }
+    S->beta = tot[1] / S->rz_old;
+    S->rz_old = tot[1];
+    S->p_pending = 1;
+  } else {
+    S->reliable_updates += 1;
+    if (PREC == FEAB_PREC_FP32) S->xsel ^= 1;
+    const double rel = sqrt(S->rr64) / S->bnorm;
+    S->relres = rel;
+    if (rel < S->tol) {
+      S->done = 1;
+      S->status = FEAB_OK;
+      return;
+    }
+    if (S->iters >= S->maxiter || !(rel == rel)) {
+      S->done = 1;
+      S->status = FEAB_NOT_CONVERGED;
+      return;
+    }
+    S->rmax = sqrt(S->rr64);
+    S->beta = tot[1] / S->rz_old;
+    S->rz_old = tot[1];
+    S->mode = kModeCG;
+    S->p_pending = 1;
+  }
+}
+
+// fp32 mode: x = x64 + x32 (the correction is zero after a final reliable step).
+__global__ void k_finalize_fp32(PcgArgs A) {
+  const double* x64 = A.S_->xsel ? A.x64b : A.x64a;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+    A.x[i] = x64[i] + (double)A.x32[i];
+}
+
+// Standalone y = A x with the step-A SpMV (same group_spmv code and launch shape).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) k_spmv(PcgArgs A, const T* __restrict__ x, T* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int G = A.group_ptr ? A.n_groups : A.n;
+  const T* vals;
+  if constexpr (sizeof(T) == 8) vals = reinterpret_cast<const T*>(A.vals64);
+  else vals = reinterpret_cast<const T*>(A.vals32);
+  for (int g = wg; g < G; g += nw) {
+    int r0, f;
+    group_rows(A, g, r0, f);
+    T acc[3];
+    group_spmv<T>(A, vals, r0, f, lane, [&](int j) { return __ldg(x + j); }, acc);
+    if (lane < f) y[r0 + lane] = pick3(acc, lane);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
+  const int lane = threadIdx.x & 31;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  for (int g = wg; g < A.n_groups; g += nw) {
+    int r0, f;
+    group_rows(A, g, r0, f);
+    double acc[3];
+    group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(x + j); }, acc);
+    if (lane < f) y[r0 + lane] = pick3(acc, lane);
+  }
+}
+
+// Difference-form operator from the FP64 CSR: tagged columns, 48-bit values, group masks and
+// the row-block sums S[r][j] = sum over the row's columns of DOF component j (fixed order).
+__global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const int32_t* __restrict__ group_ptr,
+                                                         const int32_t* __restrict__ row_ptr,
+                                                         const int32_t* __restrict__ col_idx,
+                                                         const double* __restrict__ vals,
+                                                         const int32_t* __restrict__ dof_of,
+                                                         int32_t* __restrict__ tcol, uint32_t* __restrict__ vhi,
+                                                         uint16_t* __restrict__ vlo, uint8_t* __restrict__ gmask,
+                                                         double* __restrict__ Ssum) {
+  const int lane = threadIdx.x & 31;
+  const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  if (g >= n_groups) return;
+  const int r0 = group_ptr[g], f = group_ptr[g + 1] - r0;
+  if (lane == 0) {
+    int m = 0;
+    for (int k = 0; k < f; ++k) m |= 1 << (dof_of[r0 + k] % 3);
+    gmask[g] = (uint8_t)m;
+  }
+  for (int k = 0; k < f; ++k) {
+    const int s0 = row_ptr[r0 + k], len = row_ptr[r0 + k + 1] - s0;
+    double sj[3] = {0.0, 0.0, 0.0};
+    for (int c0 = 0; c0 < len; c0 += 32) {
+      const int c = c0 + lane;
+      double v = 0.0;
+      int j = 0;
+      if (c < len) {
+        const int col = col_idx[s0 + c];
+        j = dof_of[col] % 3;
+        v = vals[s0 + c];
+        if (k == 0) tcol[s0 + c] = (int32_t)((uint32_t)col | ((uint32_t)j << 30));
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
+        vhi[s0 + c] = (uint32_t)(bits >> 32);
+        vlo[s0 + c] = (uint16_t)((bits >> 16) & 0xffffull);
+      }
+      // fixed-order per-row sums: lanes in order, chunks in order
+      for (int u = 0; u < 32; ++u) {
+        const double vu = __shfl_sync(FEAB_FULL_MASK, v, u);
+        const int ju = __shfl_sync(FEAB_FULL_MASK, j, u);
+        if (c0 + u < len) sj[ju] += vu;
+      }
+    }
+    if (lane < 3) Ssum[(int64_t)(r0 + k) * 3 + lane] = lane == 0 ? sj[0] : (lane == 1 ? sj[1] : sj[2]);
+  }
+}
+
+size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+int max_grid() { return sm_count() * 8; }
+
+struct Grids {
+  int a, b;
+};
+
+Grids grids_for(int n, int G) {
+  Grids g;
+  g.a = std::max(1, (int)std::min<int64_t>(((int64_t)G + 7) / 8, (int64_t)max_grid()));
+  g.b = std::max(1, (int)std::min<int64_t>(((int64_t)n + kThreads * 4 - 1) / (kThreads * 4), (int64_t)max_grid()));
+  return g;
+}
+
+size_t layout(int32_t n, int32_t precision, char* base, PcgArgs* A) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off += a256(bytes);
+    return base ? base + o : nullptr;
+  };
+  const size_t nd = sizeof(double) * (size_t)n, nf = sizeof(float) * (size_t)n;
+  char* s = take(sizeof(PcgState));
+  char* part = take(sizeof(double) * 2 * (size_t)max_grid());
+  if (A) {
+    A->S_ = reinterpret_cast<PcgState*>(s);
+    A->partials = reinterpret_cast<double*>(part);
+  }
+  if (precision == FEAB_PREC_FP32) {
+    char* xa = take(nd);
+    char* xb = take(nd);
+    char* r64 = take(nd);
+    char* r32 = take(nf);
+    char* z32 = take(nf);
+    char* q0 = take(nf);
+    char* q1 = take(nf);
+    char* ap32 = take(nf);
+    char* x32 = take(nf);
+    if (A) {
+      A->x64a = reinterpret_cast<double*>(xa);
+      A->x64b = reinterpret_cast<double*>(xb);
+      A->r64 = reinterpret_cast<double*>(r64);
+      A->r32 = reinterpret_cast<float*>(r32);
+      A->z32 = reinterpret_cast<float*>(z32);
+      A->q0 = reinterpret_cast<float*>(q0);
+      A->q1 = reinterpret_cast<float*>(q1);
+      A->Ap32 = reinterpret_cast<float*>(ap32);
+      A->x32 = reinterpret_cast<float*>(x32);
+    }
+  } else {
+    char* r = take(nd);
+    char* z = take(nd);
+    char* p0 = take(nd);
+    char* p1 = take(nd);
+    char* ap = take(nd);
+    if (A) {
+      A->r = reinterpret_cast<double*>(r);
+      A->z = reinterpret_cast<double*>(z);
+      A->p0 = reinterpret_cast<double*>(p0);
+      A->p1 = reinterpret_cast<double*>(p1);
+      A->Ap = reinterpret_cast<double*>(ap);
+    }
+  }
+  return off;
+}
+
+struct HostFlag {
+  volatile int32_t* ptr = nullptr;
+  HostFlag() {
+    void* p = nullptr;
+    if (cudaHostAlloc(&p, 64, cudaHostAllocDefault) == cudaSuccess) ptr = static_cast<volatile int32_t*>(p);
+  }
+  ~HostFlag() {
+    if (ptr) cudaFreeHost((void*)ptr);
+  }
+};
+
+template <int PREC>
+void launch_setup(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
+  k_setup_a<PREC><<<gr.a, kThreads, 0, s>>>(A);
+  k_setup_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
+  count_launches(2);
+}
+
+template <int PREC>
+void launch_step(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
+  k_step_a<PREC><<<gr.a, kThreads, 0, s>>>(A);
+  k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
+}
+
+int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, feab_pcg_result* result, cudaStream_t s) {
+  const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
+  static thread_local HostFlag flag;
+  if (!flag.ptr) return FEAB_CUDA_ERROR;
+  if (prec == FEAB_PREC_FP32) launch_setup<FEAB_PREC_FP32>(A, gr, s);
+  else if (prec == FEAB_PREC_MIXED) launch_setup<FEAB_PREC_MIXED>(A, gr, s);
+  else launch_setup<FEAB_PREC_FP64>(A, gr, s);
+  FEAB_CHECK_LAUNCH();
+
+  cudaStream_t cs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int32_t rc = FEAB_OK;
+  int64_t launched = 0;
+  auto fail = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == FEAB_OK) rc = FEAB_CUDA_ERROR;
+    return e != cudaSuccess;
+  };
+  do {
+    if (fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking))) break;
+    if (fail(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming))) break;
+    if (fail(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) break;
+    if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
+    for (int c = 0; c < chunk; ++c) {
+      if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, cs);
+      else if (prec == FEAB_PREC_MIXED) launch_step<FEAB_PREC_MIXED>(A, gr, cs);
+      else launch_step<FEAB_PREC_FP64>(A, gr, cs);
+    }
+    cudaMemcpyAsync((void*)flag.ptr, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
+    if (fail(cudaStreamEndCapture(cs, &graph))) break;
+    if (fail(cudaGraphInstantiate(&exec, graph, 0))) break;
+
+    // Every CG iteration is one step and a reliable step follows at most every iteration, so
+    // 2*maxiter + 2 steps always suffice: the host loop is bounded.
+    const int64_t max_launch = (2 * (int64_t)maxiter + 2 + chunk - 1) / chunk + 1;
+    flag.ptr[0] = 0;
+    if (fail(cudaGraphLaunch(exec, s))) break;
+    if (fail(cudaEventRecord(ev[0], s))) break;
+    launched = 1;
+    count_launches(2 * (uint64_t)chunk);
+    while (true) {
+      const bool more = launched < max_launch;
+      if (more) {
+        if (fail(cudaGraphLaunch(exec, s))) break;
+        if (fail(cudaEventRecord(ev[launched & 1], s))) break;
+        ++launched;
+        count_launches(2 * (uint64_t)chunk);
+      }
+      if (fail(cudaEventSynchronize(ev[more ? ((launched - 2) & 1) : ((launched - 1) & 1)]))) break;
+      if (flag.ptr[0] != 0 || !more) break;
+    }
+  } while (false);
+
+  if (rc == FEAB_OK && prec == FEAB_PREC_FP32) {
+    k_finalize_fp32<<<gr.b, kThreads, 0, s>>>(A);
+    count_launches(1);
+    fail(cudaGetLastError());
+  }
+  PcgState hs;
+  if (rc == FEAB_OK) {
+    if (!fail(cudaMemcpyAsync(&hs, A.S_, sizeof(PcgState), cudaMemcpyDeviceToHost, s))) fail(cudaStreamSynchronize(s));
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (ev[0]) cudaEventDestroy(ev[0]);
+  if (ev[1]) cudaEventDestroy(ev[1]);
+  if (cs) cudaStreamDestroy(cs);
+  if (rc != FEAB_OK) {
+    if (result) result->status = rc;
+    return rc;
+  }
+  int32_t st = hs.status;
+  if (hs.done == 0) st = FEAB_NOT_CONVERGED;
+  if (result) {
+    result->status = st;
+    result->iters = hs.iters;
+    result->reliable_updates = hs.reliable_updates;
+    result->graph_launches = (int32_t)launched;
+    result->relres = hs.relres;
+    result->bnorm = hs.bnorm;
+  }
+  return st;
+}
+
+void fill_matrix(const feab_csr* M, PcgArgs* A) {
+  A->n = M->n;
+  A->n_groups = M->n_groups;
+  A->row_ptr = M->row_ptr;
+  A->col_idx = M->col_idx;
+  A->group_ptr = M->group_ptr;
+  A->vals64 = M->vals64;
+  A->vals32 = M->vals32;
+}
+
+void fill_diff(const feab_diff_operator* D, PcgArgs* A) {
+  A->tcol = D->tcol;
+  A->vhi = D->vhi;
+  A->vlo = D->vlo;
+  A->gmask = D->gmask;
+  A->S = D->S;
+}
+
+void diff_layout(int32_t n, int64_t nnz, int32_t n_groups, char* base, feab_diff_operator* D, size_t* total) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    char* p = base ? base + off : nullptr;
+    off += a256(bytes);
+    return p;
+  };
+  char* tc = take(sizeof(int32_t) * (size_t)nnz);
+  char* hi = take(sizeof(uint32_t) * (size_t)nnz);
+  char* lo = take(sizeof(uint16_t) * (size_t)nnz);
+  char* gm = take((size_t)n_groups);
+  char* ss = take(sizeof(double) * 3 * (size_t)n);
+  if (D) {
+    D->tcol = reinterpret_cast<int32_t*>(tc);
+    D->vhi = reinterpret_cast<uint32_t*>(hi);
+    D->vlo = reinterpret_cast<uint16_t*>(lo);
+    D->gmask = reinterpret_cast<uint8_t*>(gm);
+    D->S = reinterpret_cast<double*>(ss);
+  }
+  if (total) *total = off;
+}
+
+}  // namespace
+}  // namespace feab
+
+using namespace feab;
+
+extern "C" size_t feab_pcg_workspace_bytes(int32_t n, int32_t precision) {
+  if (n < 0 || precision < FEAB_PREC_FP64 || precision > FEAB_PREC_FP32) return 0;
+  return layout(n, precision, nullptr, nullptr);
+}
+
+extern "C" size_t feab_diff_operator_bytes(int32_t n, int64_t nnz, int32_t n_groups) {
+  if (n < 0 || nnz < 0 || n_groups < 0) return 0;
+  size_t total = 0;
+  diff_layout(n, nnz, n_groups, nullptr, nullptr, &total);
+  return total;
+}
+
+extern "C" int32_t feab_diff_operator_build(const feab_csr* M, const int32_t* dof_of, void* storage,
+                                            size_t storage_bytes, feab_diff_operator* out, cudaStream_t s) {
+  if (!M || !dof_of || !storage || !out || !M->group_ptr || M->n_groups <= 0 || !M->vals64 || M->n <= 0)
+    return FEAB_BAD_ARG;
+  if (M->n >= (1 << 30)) return FEAB_CAPACITY;
+  if (feab_diff_operator_bytes(M->n, M->nnz, M->n_groups) > storage_bytes) return FEAB_BAD_ARG;
+  diff_layout(M->n, M->nnz, M->n_groups, static_cast<char*>(storage), out, nullptr);
+  const int wpb = kThreads / 32;
+  k_build_diff<<<(M->n_groups + wpb - 1) / wpb, kThreads, 0, s>>>(M->n_groups, M->group_ptr, M->row_ptr, M->col_idx,
+                                                                   M->vals64, dof_of, out->tcol, out->vhi, out->vlo,
+                                                                   out->gmask, out->S);
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
+}
+
+extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* Dop, const double* dinv64,
+                                  const float* dinv32, const double* b, const double* x0, double* x,
+                                  const feab_pcg_params* prm, void* workspace, size_t workspace_bytes,
+                                  feab_pcg_result* result, cudaStream_t s) {
+  if (!M || !prm || !b || !x || !workspace || M->n <= 0 || !M->row_ptr || !M->col_idx || !M->vals64)
+    return FEAB_BAD_ARG;
+  const int prec = prm->precision;
+  if (prec < FEAB_PREC_FP64 || prec > FEAB_PREC_FP32) return FEAB_BAD_ARG;
+  if (prec == FEAB_PREC_FP32 && !M->vals32) return FEAB_BAD_ARG;
+  if (prec == FEAB_PREC_MIXED && (!Dop || !M->group_ptr)) return FEAB_BAD_ARG;
+  if (prm->use_dinv && (prec == FEAB_PREC_FP32 ? !dinv32 : !dinv64)) return FEAB_BAD_ARG;
+  if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
+  if (!(prm->tol >= 0.0)) return FEAB_BAD_ARG;
+  PcgArgs A{};
+  if (layout(M->n, prec, static_cast<char*>(workspace), &A) > workspace_bytes) return FEAB_BAD_ARG;
+  fill_matrix(M, &A);
+  if (Dop) fill_diff(Dop, &A);
+  A.dinv64 = dinv64;
+  A.dinv32 = dinv32;
+  A.b = b;
+  A.x0 = x0;
+  A.x = x;
+  A.use_dinv = prm->use_dinv ? 1 : 0;
+  const int maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
+  const double delta = prm->reliable_delta > 0.0 && prm->reliable_delta < 1.0 ? prm->reliable_delta : 0.1;
+  const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
+  k_init_state<<<1, 1, 0, s>>>(A.S_, prm->tol, delta, maxiter);
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  if (prec == FEAB_PREC_FP32) {
+    if (x0) FEAB_CUDA(cudaMemcpyAsync(A.x64a, x0, sizeof(double) * M->n, cudaMemcpyDeviceToDevice, s));
+    else FEAB_CUDA(cudaMemsetAsync(A.x64a, 0, sizeof(double) * M->n, s));
+    FEAB_CUDA(cudaMemsetAsync(A.x32, 0, sizeof(float) * M->n, s));
+  } else if (x0) {
+    if (x0 != x) FEAB_CUDA(cudaMemcpyAsync(x, x0, sizeof(double) * M->n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    FEAB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * M->n, s));
+  }
+  return run_pcg(A, prec, chunk, maxiter, result, s);
+}
+
+extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Dop, int32_t precision, const void* x,
+                                 void* y, cudaStream_t s) {
+  if (!M || !x || !y || M->n <= 0 || !M->row_ptr || !M->col_idx) return FEAB_BAD_ARG;
+  if (precision < FEAB_PREC_FP64 || precision > FEAB_PREC_FP32) return FEAB_BAD_ARG;
+  if (precision == FEAB_PREC_FP32 ? !M->vals32 : !M->vals64) return FEAB_BAD_ARG;
+  if (precision == FEAB_PREC_MIXED && (!Dop || !M->group_ptr)) return FEAB_BAD_ARG;
+  if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
+  PcgArgs A{};
+  fill_matrix(M, &A);
+  const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
+  if (precision == FEAB_PREC_FP64) {
+    k_spmv<double><<<gr.a, kThreads, 0, s>>>(A, static_cast<const double*>(x), static_cast<double*>(y));
+  } else if (precision == FEAB_PREC_FP32) {
+    k_spmv<float><<<gr.a, kThreads, 0, s>>>(A, static_cast<const float*>(x), static_cast<float*>(y));
+  } else {
+    fill_diff(Dop, &A);
+    k_spmv_diff<<<gr.a, kThreads, 0, s>>>(A, static_cast<const double*>(x), static_cast<double*>(y));
+  }
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
+}

@@ -1,0 +1,339 @@
+"""FESystem: drop-in for fea_engine's FESystem on the hex8 linear-elastic static path.
+
+Same constructor, method names, argument meaning and exceptions as
+fea_engine/src/fea_engine/solver.py for: assemble_stiffness (:569-697), fix_dofs
+(:1109-1176), add_nodal_force (:1178-1206), add_consistent_facet_load (:1229-1274),
+free_dofs / fixed_dofs_array (:1400-1401, :1482-1487), form_linear_system (:1403-1441) and
+solve_static (:1726-2038).  Assembly and the solve run in libfeab200 on the GPU; the load
+vector F and the boundary-condition bookkeeping stay host-side numpy, as in the reference.
+
+Differences, by design:
+- Hex8Solid3D, single block, method="full" only (others raise NotImplementedError).
+- solve_static(method=None) (the reference's SuperLU direct solve) runs the FP64 Jacobi-PCG
+  to a relative residual of 1e-12 instead; there is no direct factorisation on this path.
+- ``K`` (the full matrix, built on first access) is the structural CSR: entries that cancel to
+  exactly 0.0 are kept, where the reference's LIL storage drops them.
+- Extra keyword ``precision="fp64"|"mixed"|"fp32"`` on solve_static selects the PCG precision
+  (libfeab200's FEAB_PREC_*); every choice converges on the FP64 residual.
+"""
+from __future__ import annotations
+
+import time
+import warnings
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .device import DeviceMesh, DeviceStatus, cuda_device, pcg_solve
+from .elements import is_hex8
+from .facet_loads import facet_load_shares_batch
+from .fields import FEField
+
+
+class FESystem:
+    def __init__(self, mesh, elem_formulation, thickness=1.0, sparse=False, backend="scipy", device="cpu"):
+        if backend not in ("scipy", "torch", "auto"):
+            raise ValueError(f"FESystem: unknown backend={backend!r} -- expected 'scipy', 'torch' or 'auto'.")
+        if isinstance(elem_formulation, dict):
+            raise NotImplementedError("FESystem: multi-block meshes are not supported on the hex8 GPU path")
+        if not is_hex8(elem_formulation):
+            raise NotImplementedError(
+                f"FESystem: only Hex8Solid3D is implemented on the GPU path, got {type(elem_formulation).__name__}")
+        nodes = np.asarray(mesh.nodes, dtype=float)
+        if nodes.ndim != 2 or nodes.shape[1] != 3:
+            raise ValueError("FESystem: a hex8 solid mesh needs 3-D node coordinates")
+        self.mesh = mesh
+        self.elem = elem_formulation
+        self.thickness = thickness
+        self.sparse = sparse
+        self.backend = backend
+        self.device_name = device
+        self.npn = 3
+        self.n_dof = 3 * len(nodes)
+        self.F = np.zeros(self.n_dof)
+        self.fixed_dofs = set()
+        self.fixed_dof_values = {}
+        self._assembled = set()
+        self._warned_reassembly = set()
+        self._dmesh = None
+        self._ke = None          # packed element matrices on the device (E, 324)
+        self._ke_version = 0
+        self._op_cache = None    # (key, ReducedOperator)
+        self._K_full = None
+        self._stiffness_args = None
+        self.last_solve_info = None
+
+    # ------------------------------------------------------------------ device objects
+    @property
+    def device(self):
+        return self.device_mesh.device
+
+    @property
+    def device_mesh(self) -> DeviceMesh:
+        if self._dmesh is None:
+            self._dmesh = DeviceMesh(self.mesh.nodes, self.mesh.elements, device=cuda_device(self.device_name))
+        return self._dmesh
+
+    # ------------------------------------------------------------------ named DOFs
+    @property
+    def dof_names(self):
+        return ("ux", "uy", "uz")
+
+    def dof_index(self, name):
+        return self._dof_index_by_name(name, "dof_index")
+
+    def _dof_index_by_name(self, name, who):
+        low = [n.lower() for n in self.dof_names]
+        if str(name).lower() in low:
+            return low.index(str(name).lower())
+        raise ValueError(f"{who}: unknown DOF name {name!r}; valid names: {list(self.dof_names)}.")
+
+    # ------------------------------------------------------------------ input validation
+    @staticmethod
+    def _as_int_array(values, what, who):
+        arr = np.asarray(list(values) if isinstance(values, (set, frozenset)) else values).reshape(-1)
+        if arr.size and arr.dtype.kind not in "iu":
+            if arr.dtype.kind == "f" and np.all(arr == np.round(arr)):
+                arr = arr.astype(int)
+            else:
+                raise ValueError(f"{who}: {what} must be integers, got {arr.dtype}.")
+        return arr.astype(int)
+
+    def _check_nodes(self, node_ids, who):
+        if isinstance(node_ids, str) or (isinstance(node_ids, (list, tuple)) and node_ids
+                                         and all(isinstance(n, str) for n in node_ids)):
+            names = [node_ids] if isinstance(node_ids, str) else list(node_ids)
+            sets = getattr(self.mesh, "node_sets", {})
+            missing = [n for n in names if n not in sets]
+            if missing:
+                raise ValueError(f"{who}: unknown node set(s) {missing}; available: {sorted(sets)}.")
+            node_ids = np.unique(np.concatenate([np.asarray(sets[n], dtype=int) for n in names]))
+        nodes = self._as_int_array(node_ids, "node ids", who)
+        if nodes.size == 0:
+            raise ValueError(f"{who}: no nodes selected (node_ids is empty).")
+        n_nodes = len(self.mesh.nodes)
+        bad = nodes[(nodes < 0) | (nodes >= n_nodes)]
+        if bad.size:
+            raise ValueError(f"{who}: node id(s) {sorted(set(bad.tolist()))[:5]} outside the mesh "
+                             f"(valid range 0..{n_nodes - 1}).")
+        return nodes
+
+    def _check_local_dofs(self, dof_indices, who):
+        if isinstance(dof_indices, (set, frozenset)):
+            items = list(dof_indices)
+        elif isinstance(dof_indices, str) or np.ndim(dof_indices) == 0:
+            items = [dof_indices]
+        else:
+            items = list(dof_indices)
+        resolved = [self._dof_index_by_name(it, who) if isinstance(it, str) else it for it in items]
+        dofs = self._as_int_array(np.array(resolved), "local DOF indices", who)
+        if dofs.size == 0:
+            raise ValueError(f"{who}: no DOF indices given.")
+        bad = dofs[(dofs < 0) | (dofs >= self.npn)]
+        if bad.size:
+            raise ValueError(f"{who}: local DOF index {sorted(set(bad.tolist()))} is out of range -- "
+                             f"Hex8Solid3D has 3 DOF(s) per node, so valid indices are 0..2.")
+        return dofs
+
+    # ------------------------------------------------------------------ assembly
+    def assemble_stiffness(self, D, method="full", vectorized=False, accumulate=False, **kwargs):
+        """Element matrices on the GPU (ke = sum_gp B^T D B detJ w thickness), kept packed on
+        the device; the reduced CSR is assembled for the current boundary conditions at solve
+        time.  ``vectorized`` is accepted for signature compatibility (every path is batched)."""
+        if method not in ("full", "reduced", "hourglass_stabilized"):
+            raise ValueError(f"assemble_stiffness: unknown method={method!r} -- expected "
+                             f"'full' (default), 'reduced', or 'hourglass_stabilized'.")
+        if method != "full":
+            raise NotImplementedError("assemble_stiffness: only method='full' is implemented on the GPU path")
+        gauss_order = kwargs.pop("gauss_order", None)
+        thickness = kwargs.pop("thickness", 1.0)
+        kwargs.pop("chunk_size", None)
+        kwargs.pop("backend", None)
+        kwargs.pop("device", None)
+        if kwargs:
+            raise TypeError(f"assemble_stiffness: unsupported kwargs {list(kwargs)} -- only gauss_order=/thickness=/"
+                            f"chunk_size=/backend=/device= are accepted.")
+        if gauss_order not in (None, 2):
+            raise NotImplementedError("assemble_stiffness: only the full 2x2x2 Gauss rule is implemented")
+        if isinstance(D, dict):
+            if len(D) != 1:
+                raise NotImplementedError("assemble_stiffness: per-block D needs a multi-block mesh")
+            D = next(iter(D.values()))
+        D = np.asarray(D, dtype=float)
+        if D.shape != (6, 6):
+            raise ValueError(f"D has shape {D.shape} but Hex8Solid3D's B matrix has 6 strain rows -- "
+                             f"mismatched material/element pair.")
+        if not np.allclose(D, D.T, rtol=1e-12, atol=0.0):
+            raise ValueError("assemble_stiffness: D must be symmetric (the PCG path needs an SPD K)")
+        if "K" in self._assembled and not accumulate and "K" not in self._warned_reassembly:
+            warnings.warn("assemble_stiffness: K was already assembled, so it is being REPLACED. Pass "
+                          "accumulate=True to add to the existing matrix instead.", UserWarning, stacklevel=2)
+            self._warned_reassembly.add("K")
+        ke = self.device_mesh.element_stiffness(D, thickness=thickness)
+        if accumulate and self._ke is not None:
+            self._ke = self._ke + ke
+        else:
+            self._ke = ke
+        self._ke_version += 1
+        self._op_cache = None
+        self._K_full = None
+        self._assembled.add("K")
+        self._stiffness_args = (D, {"thickness": thickness})
+
+    def _require_stiffness(self, who):
+        if self._ke is None:
+            raise RuntimeError(f"{who}: the global stiffness matrix K is all zeros -- call "
+                               f"assemble_stiffness(...) before solving.")
+
+    # ------------------------------------------------------------------ boundary conditions / loads
+    def fix_dofs(self, node_ids, dof_indices, value=0.0):
+        nodes = self._check_nodes(node_ids, "fix_dofs")
+        dofs = self._check_local_dofs(dof_indices, "fix_dofs")
+        for n in nodes:
+            for k in dofs:
+                dof = self.npn * int(n) + int(k)
+                self.fixed_dofs.add(dof)
+                self.fixed_dof_values[dof] = float(value)
+
+    def add_nodal_force(self, node_ids, dof_index, total_force):
+        nodes = self._check_nodes(node_ids, "add_nodal_force")
+        dof = int(self._check_local_dofs(dof_index, "add_nodal_force")[0])
+        share = total_force / len(nodes)
+        for n in nodes:
+            self.F[self.npn * int(n) + dof] += share
+
+    def add_consistent_facet_load(self, formulation, facets, dof_index, traction, quad_order=2, thickness=1.0):
+        facets = np.asarray([tuple(f) for f in facets], dtype=int)
+        if facets.ndim != 2 or facets.shape[1] != 4:
+            raise ValueError("add_consistent_facet_load: hex8 facets are 4-node tuples")
+        self._check_nodes(facets.reshape(-1), "add_consistent_facet_load")
+        dof_index = int(self._check_local_dofs(dof_index, "add_consistent_facet_load")[0])
+        shares = facet_load_shares_batch(np.asarray(self.mesh.nodes)[facets], traction * thickness, quad_order)
+        np.add.at(self.F, self.npn * facets.reshape(-1) + dof_index, shares.reshape(-1))
+
+    @property
+    def free_dofs(self):
+        mask = np.ones(self.n_dof, dtype=bool)
+        if self.fixed_dofs:
+            mask[np.fromiter(self.fixed_dofs, dtype=np.int64)] = False
+        return np.flatnonzero(mask)
+
+    @property
+    def fixed_dofs_array(self):
+        return np.array(sorted(self.fixed_dofs), dtype=int)
+
+    def _fixed_dof_values_array(self, fixed):
+        return np.array([self.fixed_dof_values.get(int(d), 0.0) for d in fixed])
+
+    # ------------------------------------------------------------------ reduced operator
+    def reduced_operator(self, want32=True):
+        """K_ff for the current fixed set on the device (cached until K or the BCs change)."""
+        self._require_stiffness("reduced_operator")
+        fixed = self.fixed_dofs_array
+        key = (self._ke_version, fixed.tobytes(), bool(want32))
+        if self._op_cache is not None and self._op_cache[0] == key:
+            return self._op_cache[1]
+        dm = self.device_mesh
+        pat = dm.pattern(fixed)
+        op = dm.assemble(self._ke, pat, want32=want32)
+        self._op_cache = (key, op)
+        return op
+
+    def _reduced_rhs(self, F=None):
+        """F_f - K[free, fixed] u_fixed as a device vector (solver.py:1496-1511)."""
+        Fv = self.F if F is None else np.asarray(F, dtype=float)
+        free = self.free_dofs
+        fixed = self.fixed_dofs_array
+        u_fixed = self._fixed_dof_values_array(fixed)
+        Ff = torch.as_tensor(np.ascontiguousarray(Fv[free])).to(self.device)
+        if fixed.size and np.any(u_fixed):
+            v = np.zeros(self.n_dof)
+            v[fixed] = u_fixed
+            y = self.device_mesh.apply(self._ke, v)
+            Ff = Ff - y[torch.as_tensor(free).to(self.device)]
+        return Ff
+
+    @property
+    def K(self):
+        """Full (n_dof x n_dof) stiffness as a host scipy CSR (structural pattern)."""
+        self._require_stiffness("K")
+        if self._K_full is None:
+            dm = self.device_mesh
+            pat = dm.pattern(())
+            self._K_full = dm.assemble(self._ke, pat, want32=False).to_scipy()
+        return self._K_full
+
+    def field(self, data, label=None):
+        if not isinstance(data, np.ndarray) or data.ndim not in (1, 2) or data.shape[0] != self.n_dof:
+            return data
+        return FEField(data, n_nodes=len(self.mesh.nodes), dofs_per_node=3, dof_names=self.dof_names, label=label,
+                       mesh=self.mesh)
+
+    # ------------------------------------------------------------------ solve
+    def solve_static(self, verbose=False, method=None, **method_kwargs):
+        U = self.solve_static_device(verbose=verbose, method=method, **method_kwargs)
+        return self.field(U.cpu().numpy(), label="displacement")
+
+    def solve_static_device(self, verbose=False, method=None, **method_kwargs):
+        """solve_static, returning the full displacement vector as a device tensor."""
+        self._require_stiffness("solve_static")
+        fixed = self.fixed_dofs_array
+        u_fixed = self._fixed_dof_values_array(fixed)
+        if not np.any(self.F) and not np.any(u_fixed):
+            warnings.warn("solve_static: the load vector F is all zeros and no non-zero displacement is "
+                          "prescribed, so the solution is trivially zero.", UserWarning, stacklevel=3)
+        if method not in (None, "cg", "pcg"):
+            raise ValueError(f"solve_static: unknown method={method!r} -- choose from 'cg', 'pcg' (or None).")
+        kw = dict(method_kwargs)
+        precision = kw.pop("precision", "fp64")
+        delta = kw.pop("reliable_delta", 0.1)
+        precond = kw.pop("preconditioner", "jacobi")
+        kw.pop("omega", None)
+        if method == "pcg" and precond != "jacobi":
+            if precond in ("ssor", "ic0"):
+                raise NotImplementedError(f"solve_static(method='pcg', preconditioner={precond!r}): only 'jacobi' "
+                                          f"is implemented on the GPU path")
+            raise ValueError(f"solve_static(method='pcg'): unknown preconditioner={precond!r} -- choose 'jacobi', "
+                             f"'ssor', or 'ic0'.")
+        tol = kw.pop("tol", 1e-12 if method is None else 1e-8)
+        maxiter = kw.pop("maxiter", None)
+        x0 = kw.pop("x0", None)
+        if kw:
+            raise TypeError(f"solve_static: unsupported keyword(s) {sorted(kw)}")
+        t0 = time.perf_counter()
+        op = self.reduced_operator(want32=(precision == "fp32"))
+        Ff = self._reduced_rhs()
+        x, info = pcg_solve(op, Ff, x0=x0, tol=tol, maxiter=maxiter, precision=precision,
+                            use_dinv=(method != "cg"), reliable_delta=delta)
+        self.last_solve_info = info
+        if info.status == L.FEAB_NOT_SPD:
+            raise np.linalg.LinAlgError("preconditioned_cg: p^T A p <= 0 -- A is not SPD.")
+        if info.status == L.FEAB_NOT_CONVERGED:
+            raise RuntimeError(f"preconditioned_cg: did not converge in {info.iters} iterations "
+                               f"(final relative residual {info.relres:.3e} >= tol={tol:.1e}).")
+        L.raise_for(info.status, "solve_static")
+        U = torch.zeros(self.n_dof, dtype=torch.float64, device=self.device)
+        free_t = torch.as_tensor(self.free_dofs).to(self.device)
+        U[free_t] = x
+        if fixed.size:
+            U[torch.as_tensor(fixed).to(self.device)] = torch.as_tensor(u_fixed).to(self.device)
+        if verbose:
+            print(f"[feab200] n={op.n} nnz={op.nnz} precision={precision} iters={info.iters} "
+                  f"relres={info.relres:.3e} reliable_updates={info.reliable_updates} "
+                  f"time={time.perf_counter() - t0:.3f}s")
+        return U
+
+    def form_linear_system(self, F=None, K=None):
+        from .linear_system import ReducedSystem
+        if K is not None:
+            raise NotImplementedError("form_linear_system: a caller-supplied K is not supported on the GPU path")
+        self._require_stiffness("form_linear_system")
+        Fv = self.F if F is None else np.asarray(F, dtype=float)
+        if Fv.shape != (self.n_dof,):
+            raise ValueError(f"F must have shape ({self.n_dof},), got {Fv.shape}")
+        fixed = self.fixed_dofs_array
+        op = self.reduced_operator()
+        Ff = self._reduced_rhs(Fv)
+        return ReducedSystem(operator=op, F_device=Ff, free=self.free_dofs, fixed=fixed,
+                             u_fixed=self._fixed_dof_values_array(fixed), n_dof=self.n_dof, _system=self)

@@ -1,0 +1,219 @@
+/*
+ * feab200 -- C ABI of the B200 (sm_100a) hex8 linear-elastic library.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, and returns an
+ * int status (FEAB_OK on success).  Pointers named d_* / device arrays are device
+ * memory owned by the caller; the library never frees caller memory.  Scratch memory
+ * is passed in by the caller (sizes from the *_bytes queries), so the library itself
+ * performs no cudaMalloc.  Work is enqueued on the given stream; functions documented
+ * as "synchronous" also wait for it and read small results back to the host.
+ *
+ * Device-side failures (degenerate element, zero diagonal, capacity) are written to a
+ * caller-provided feab_device_status in device memory: the first failure wins and
+ * records the offending element/node/row index.
+ *
+ * The reference (abhi2k16/computation-suite, fea_engine) is pure Python; each entry
+ * point names the reference function whose work it replaces (file:line inside
+ * fea_engine/src/fea_engine/ unless stated).
+ */
+#ifndef FEAB200_H
+#define FEAB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (map to the reference's Python exceptions, see the Python layer) ---- */
+#define FEAB_OK 0
+#define FEAB_BAD_ARG 1              /* ValueError  (bad sizes / indices)                   */
+#define FEAB_DEGENERATE_ELEMENT 2   /* ValueError  mesh_transform.py:327-332 (|detJ|<1e-300) */
+#define FEAB_ZERO_DIAGONAL 3        /* ValueError  iterative_solvers.py:199-200            */
+#define FEAB_NOT_SPD 4              /* LinAlgError iterative_solvers.py:450-454 (pAp <= 0) */
+#define FEAB_NOT_CONVERGED 5        /* RuntimeError iterative_solvers.py:478-481           */
+#define FEAB_CUDA_ERROR 6           /* RuntimeError (CUDA launch / runtime failure)        */
+#define FEAB_CAPACITY 7             /* ValueError  node valence beyond the kernels' limit  */
+
+#define FEAB_HEX8_KE_PACKED 324     /* doubles per element: the 36 upper 3x3 node blocks   */
+#define FEAB_HEX8_KE_FULL 576       /* doubles per element: full 24x24, row major          */
+#define FEAB_MAX_NODE_ELEMS 64      /* elements per node supported by the topology kernels */
+#define FEAB_MAX_NODE_NBRS 128      /* distinct neighbour nodes per node                   */
+
+typedef struct feab_device_status {
+  int32_t code;      /* 0 = OK, else the first FEAB_* failure */
+  int32_t reserved;
+  int64_t index;     /* element / node / row that failed */
+} feab_device_status;
+
+/* Reduced stiffness in CSR form.  Rows of one mesh node share one column pattern; a
+ * group is a run of consecutive rows with identical col_idx (group_ptr may be NULL:
+ * every row is then its own group). */
+typedef struct feab_csr {
+  int32_t n;                 /* rows = columns                     */
+  int32_t n_groups;          /* groups in group_ptr (ignored if NULL) */
+  int64_t nnz;
+  const int32_t* row_ptr;    /* n+1                                */
+  const int32_t* col_idx;    /* nnz, sorted within each row        */
+  const double* vals64;      /* nnz                                */
+  const float* vals32;       /* nnz, FP32 copy (mixed precision) or NULL */
+  const int32_t* group_ptr;  /* n_groups+1 or NULL                 */
+} feab_csr;
+
+#define FEAB_PREC_FP64 0     /* plain FP64 PCG: the reference recurrence, FP64 throughout        */
+#define FEAB_PREC_MIXED 1    /* FP64 vectors/scalars; SpMV on 48-bit values in difference form;   */
+                             /* FP64 reliable residual replacement (needs a feab_diff_operator)  */
+#define FEAB_PREC_FP32 2     /* FP32 values and p/r/Ap/x-correction, FP64 scalars, FP64 reliable */
+                             /* residual replacement folding into an FP64 solution               */
+
+/* Difference-form operator built from the FP64 CSR by feab_diff_operator_build (storage is
+ * caller memory, feab_diff_operator_bytes).  Applies y_a = sum_{b!=a} K_ab (x_b - x_a) + S_a x_a
+ * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64. */
+typedef struct feab_diff_operator {
+  int32_t* tcol;     /* nnz: column | (DOF component << 30)             */
+  uint32_t* vhi;     /* nnz: upper 32 bits of the rounded double       */
+  uint16_t* vlo;     /* nnz: next 16 bits                              */
+  uint8_t* gmask;    /* n_groups: free-DOF mask of the group's node    */
+  double* S;         /* 3 n: row-block sums per DOF component          */
+} feab_diff_operator;
+
+typedef struct feab_pcg_params {
+  double tol;                /* on ||b - A x|| / ||b||  (||b|| := 1 when b == 0)          */
+  int32_t maxiter;           /* <= 0: 10 n, as iterative_solvers.py:393-394              */
+  int32_t precision;         /* FEAB_PREC_*                                              */
+  double reliable_delta;     /* mixed: FP64 residual replacement when ||r|| < delta*rmax  */
+  int32_t chunk;             /* iterations per CUDA-graph launch (<= 0: default 16)      */
+  int32_t use_dinv;          /* 1: Jacobi preconditioner (method="pcg"), 0: plain CG     */
+} feab_pcg_params;
+
+typedef struct feab_pcg_result {
+  int32_t status;            /* FEAB_OK / FEAB_NOT_SPD / FEAB_NOT_CONVERGED / ...        */
+  int32_t iters;             /* CG iterations (the reference's n_iter)                   */
+  int32_t reliable_updates;  /* mixed: FP64 residual replacements performed              */
+  int32_t graph_launches;    /* CUDA-graph replays (each holds 3*chunk kernels)          */
+  double relres;             /* final ||r||/||b|| (mixed: the FP64 true residual)        */
+  double bnorm;
+} feab_pcg_result;
+
+/* ---------------------------------------------------------------- library */
+int32_t feab_abi_version(void);
+const char* feab_status_string(int32_t code);
+/* Make `device` current for this host thread in the library's own CUDA runtime (the
+ * library links the runtime statically; its current device is independent of the caller's). */
+int32_t feab_set_device(int32_t device);
+/* Kernels this library has launched in this process (graph replays count their kernels). */
+uint64_t feab_launch_count(void);
+
+/* ---------------------------------------------------------------- topology
+ * Replaces the pattern part of scatter_global_stiffness' COO->CSR + [ix_(free,free)]
+ * (vectorized_assembly.py:217-262, solver.py:1977-1978).  The resulting row_ptr/col_idx
+ * equal SciPy's sorted int32 CSR of the reduced matrix bit for bit. */
+
+/* Scratch bytes needed by the topology calls for a mesh of this size. */
+size_t feab_topology_scratch_bytes(int32_t n_nodes, int64_t n_elem);
+
+/* Node -> element incidence, each node's list sorted by element id.
+ * conn: n_elem*8 int32 node ids.  inc_ptr: n_nodes+1, inc_elem: 8*n_elem.
+ * Synchronous: *max_elems_out = largest node valence (FEAB_CAPACITY if above
+ * FEAB_MAX_NODE_ELEMS). */
+int32_t feab_node_incidence(const int32_t* conn, int64_t n_elem, int32_t n_nodes, int32_t* inc_ptr,
+                            int32_t* inc_elem, void* scratch, size_t scratch_bytes,
+                            feab_device_status* status, int32_t* max_elems_out, cudaStream_t stream);
+
+/* Sorted node adjacency (a node is its own neighbour).  Call with nbr_idx == NULL to
+ * fill nbr_ptr (n_nodes+1) and get *total_out / *max_nbrs_out (synchronous), then again
+ * with nbr_idx (total entries) to fill it. */
+int32_t feab_node_adjacency(const int32_t* conn, const int32_t* inc_ptr, const int32_t* inc_elem,
+                            int32_t n_nodes, int32_t* nbr_ptr, int32_t* nbr_idx, void* scratch,
+                            size_t scratch_bytes, feab_device_status* status, int64_t* total_out,
+                            int32_t* max_nbrs_out, cudaStream_t stream);
+
+/* CSR pattern of the free x free block.  free_map[3*node+k] = reduced row of that DOF or
+ * -1 when fixed (fix_dofs, solver.py:1109-1176).  Call with col_idx == NULL to fill
+ * row_ptr (n_free+1) and group_ptr (n_groups+1, may be NULL) and get *nnz_out,
+ * *n_groups_out (synchronous); then again with col_idx to fill the columns. */
+int32_t feab_csr_pattern(const int32_t* nbr_ptr, const int32_t* nbr_idx, int32_t n_nodes,
+                         const int32_t* free_map, int32_t n_free, int32_t* row_ptr,
+                         int32_t* group_ptr, int32_t* col_idx, void* scratch, size_t scratch_bytes,
+                         int64_t* nnz_out, int32_t* n_groups_out, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- element kernel
+ * ke = sum over the 2x2x2 Gauss points of B^T D B detJ w (signed detJ), per element,
+ * times scale[e] when scale != NULL.  Replaces Hex8Solid3D.stiffness / B_matrix
+ * (elements/base.py:494-514, elements/solids.py:130-163) and the batched
+ * MeshTransformation + tensorized_element_stiffness einsum (mesh_transform.py:280-437,
+ * vectorized_assembly.py:165-214).  D: 36 doubles in HOST memory (symmetric 6x6, Voigt
+ * xx,yy,zz,xy,yz,zx).  layout: FEAB_HEX8_KE_PACKED (36 upper node blocks (a<=b), block
+ * (a,b) at a*8-a*(a-1)/2+(b-a), each 3x3 row major) or FEAB_HEX8_KE_FULL. */
+int32_t feab_hex8_element_stiffness(const double* coords, const int32_t* conn, int64_t n_elem,
+                                    const double* D_host, const double* scale, double thickness,
+                                    double* ke_out, int32_t layout, feab_device_status* status,
+                                    cudaStream_t stream);
+
+/* ---------------------------------------------------------------- assembly
+ * Deterministic gather assembly of the reduced CSR values from packed element
+ * matrices: each entry is summed over its elements in ascending element order.
+ * Also writes the FP32 copy (vals32 may be NULL) and the Jacobi inverse diagonal
+ * 1/diag (dinv64/dinv32 may be NULL; zero diagonal -> FEAB_ZERO_DIAGONAL).
+ * Replaces the COO duplicate summation of scatter_global_stiffness
+ * (vectorized_assembly.py:254-262) / the LIL scatter (solver.py:684-697) and
+ * jacobi_preconditioner (iterative_solvers.py:193-202). */
+int32_t feab_assemble_csr(const double* ke_packed, const int32_t* conn, const int32_t* inc_ptr,
+                          const int32_t* inc_elem, const int32_t* nbr_ptr, const int32_t* nbr_idx,
+                          int32_t n_nodes, int32_t max_nbrs, const int32_t* free_map,
+                          const int32_t* row_ptr, double* vals64, float* vals32, double* dinv64,
+                          float* dinv32, feab_device_status* status, cudaStream_t stream);
+
+/* y = K v over all 3*n_nodes DOFs, element by element from packed element matrices
+ * (node-centric gather, deterministic).  Used for the Dirichlet RHS correction
+ * F_f - K[free,fixed] u_fixed (solver.py:1496-1511) and for residual checks. */
+int32_t feab_hex8_apply(const double* ke_packed, const int32_t* conn, const int32_t* inc_ptr,
+                        const int32_t* inc_elem, int32_t n_nodes, const double* v, double* y,
+                        cudaStream_t stream);
+
+/* ---------------------------------------------------------------- PCG
+ * Jacobi-preconditioned CG, the recurrence of preconditioned_cg
+ * (iterative_solvers.py:362-481) and _cg_torch (torch_sparse_solver.py:165-202).
+ * FEAB_PREC_FP64 follows the reference step for step in FP64.  The other precisions declare
+ * convergence only on an FP64 residual b - K x computed with the FP64 values.
+ * Synchronous: returns when the solve has finished; *result holds the outcome. */
+size_t feab_pcg_workspace_bytes(int32_t n, int32_t precision);
+
+size_t feab_diff_operator_bytes(int32_t n, int64_t nnz, int32_t n_groups);
+
+/* dof_of[r] = original DOF of reduced row r (free_dofs, solver.py:1400-1401).  A needs
+ * group_ptr. */
+int32_t feab_diff_operator_build(const feab_csr* A, const int32_t* dof_of, void* storage, size_t storage_bytes,
+                                 feab_diff_operator* out, cudaStream_t stream);
+
+int32_t feab_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const double* dinv64,
+                       const float* dinv32, const double* b, const double* x0, double* x,
+                       const feab_pcg_params* params, void* workspace, size_t workspace_bytes,
+                       feab_pcg_result* result, cudaStream_t stream);
+
+/* y = A x with the PCG's SpMV kernel (same code and launch shape as one PCG step's SpMV).
+ * FEAB_PREC_FP64: x, y double, vals64; FEAB_PREC_FP32: x, y float, vals32;
+ * FEAB_PREC_MIXED: x, y double, difference form (diff != NULL).
+ * Replaces the CSR SpMV `A @ p` of preconditioned_cg (iterative_solvers.py:448) /
+ * `K_t @ x` of torch_sparse_cg_solve (torch_sparse_solver.py:255-256). */
+int32_t feab_csr_spmv(const feab_csr* A, const feab_diff_operator* diff, int32_t precision, const void* x, void* y,
+                      cudaStream_t stream);
+
+/* ---------------------------------------------------------------- SIMP adjoint
+ * out[e] = -p (1-rho_min) rho_e^(p-1) * lam_e^T K0_e u_e, with K0_e recomputed from the
+ * coordinates and D (unit modulus) at the Gauss points as sum_q eps(lam)^T D eps(u)
+ * detJ w.  lam == u gives the compliance sensitivity dC/drho
+ * (compliance_sensitivity_closed_form, topopt.py:161-177, simp_scale_grad :85-93);
+ * a general lam (an adjoint solution) gives the VJP of rho -> K(rho) u used by
+ * compliance_sensitivity_via_adjoint (topopt.py:180-232).  u, lam: 3*n_nodes. */
+int32_t feab_hex8_simp_vjp(const double* coords, const int32_t* conn, int64_t n_elem,
+                           const double* D_host, const double* rho, double penal, double rho_min,
+                           const double* u, const double* lam, double* out,
+                           feab_device_status* status, cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FEAB200_H */

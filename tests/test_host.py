@@ -1,0 +1,88 @@
+"""Host-side logic (no GPU): mesh numbering, loads, boundary-condition bookkeeping."""
+import numpy as np
+import pytest
+
+import oracle as O
+from feab200 import cantilever as cl
+from feab200 import facet_loads as fl
+from feab200.mesh import box_mesh
+from feab200.solver import FESystem
+from feab200.elements import Hex8Solid3D
+
+
+@pytest.mark.parametrize("shape", [(1, 1, 1), (3, 2, 5), (20, 4, 4), (7, 3, 2)])
+def test_box_mesh_matches_oracle(shape):
+    m = box_mesh(2.0, 0.4, 0.3, *shape)
+    nodes, el = O.box_mesh(2.0, 0.4, 0.3, *shape)
+    assert np.array_equal(m.nodes, nodes) and np.array_equal(m.elements, el)
+
+
+def test_config1_inputs_match_reference(golden):
+    g = golden("cantilever_20x4x4")
+    c = cl.plain_cantilever()
+    assert np.array_equal(c.mesh.nodes, g["nodes"])
+    assert np.array_equal(c.mesh.elements, g["elements"])
+    assert np.array_equal(c.fixed, g["fixed"])
+    assert np.abs(c.F - g["F"]).max() <= 1e-12 * np.abs(g["F"]).max()
+    assert np.isclose(c.F.sum(), -1.0e6 * 0.4 * 0.4)
+    faces = fl.boundary_faces_on_plane(c.mesh.nodes, c.mesh.elements, 0, 2.0)
+    assert np.array_equal(faces, g["facets"])
+
+
+def test_facet_batch_matches_reference(golden):
+    g = golden("facets")
+    sh = np.stack([fl.consistent_facet_load_shares(3, c, float(g["traction"])) for c in g["coords"]])
+    assert np.abs(sh - g["shares"]).max() / np.abs(g["shares"]).max() < 1e-13
+    M = np.stack([fl.consistent_facet_mass(3, c, 1.0) for c in g["coords"]])
+    assert np.abs(M - g["mass"]).max() < 1e-15
+
+
+def test_nodal_tip_load_is_consistent():
+    m = box_mesh(2.0, 0.4, 0.4, 4, 3, 3)
+    tip = m.nodes_on_plane(0, 2.0)
+    t = np.zeros(len(m.nodes))
+    t[tip] = 1.0
+    F = cl.nodal_tip_load(m, 2.0, t)
+    assert np.isclose(F.sum(), 0.4 * 0.4)           # unit traction integrates to the face area
+    assert np.allclose(F, cl.uniform_tip_load(m, 2.0, 1.0))
+
+
+def test_fesystem_bookkeeping_without_gpu(golden):
+    g = golden("cantilever_20x4x4")
+    c = cl.plain_cantilever()
+    fs = FESystem(c.mesh, Hex8Solid3D(), sparse=True)
+    fs.fix_dofs(c.mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+    assert np.array_equal(fs.fixed_dofs_array, g["fixed"])
+    assert np.array_equal(fs.free_dofs, g["free"])
+    fs.add_consistent_facet_load(Hex8Solid3D(), [tuple(f) for f in g["facets"]], 2, -1.0e6)
+    assert np.abs(fs.F - g["F"]).max() <= 1e-12 * np.abs(g["F"]).max()
+    fs.add_nodal_force([0, 1], "uy", 10.0)
+    assert fs.F[1] == 5.0 and fs.F[4] == 5.0
+
+
+def test_fesystem_argument_errors_match_reference():
+    m = box_mesh(1.0, 1.0, 1.0, 2, 2, 2)
+    with pytest.raises(ValueError):
+        FESystem(m, Hex8Solid3D(), backend="jax")
+    fs = FESystem(m, Hex8Solid3D())
+    with pytest.raises(ValueError):
+        fs.fix_dofs([], [0])
+    with pytest.raises(ValueError):
+        fs.fix_dofs([0], [3])
+    with pytest.raises(ValueError):
+        fs.fix_dofs([10_000], [0])
+    with pytest.raises(ValueError):
+        fs.add_nodal_force([0], "rx", 1.0)
+    with pytest.raises(RuntimeError):
+        fs.solve_static(method="pcg")     # K never assembled
+
+
+def test_batch_and_snapshot_builders_are_seeded():
+    a = cl.batch_cantilevers(n_problems=3, seed=9)
+    b = cl.batch_cantilevers(n_problems=3, seed=9)
+    for p, q in zip(a, b):
+        assert p.meta["shape"] == q.meta["shape"] and np.array_equal(p.F, q.F)
+        assert 4 <= p.F.shape[1] <= 16
+    s = cl.fourier_snapshot_cantilever(nx=4, ny=3, nz=3, n_rhs=5)
+    tip_t = s.F[2::3]
+    assert s.F.shape == (3 * len(s.mesh.nodes), 5) and np.abs(tip_t).max() > 0

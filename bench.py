@@ -244,13 +244,15 @@ def spmv_roofline(op, precision, reps, peak_gbs):
     x = torch.randn(op.n, dtype=dt, device=dev)
     y = torch.empty(op.n, dtype=dt, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    spmv(op, x, precision, out=y)
+    from feab200.device import tuned_lanes_per_group
+    lpg = tuned_lanes_per_group(op, precision)
+    spmv(op, x, precision, out=y, lanes_per_group=lpg)
     times = []
     for _ in range(reps):
         flush.fill_(1.0)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        spmv(op, x, precision, out=y)
+        spmv(op, x, precision, out=y, lanes_per_group=lpg)
         b.record()
         torch.cuda.synchronize()
         times.append(a.elapsed_time(b) * 1e-3)
@@ -262,7 +264,8 @@ def spmv_roofline(op, precision, reps, peak_gbs):
     kern = {"fp64": "k_spmv<double>", "fp32": "k_spmv<float>", "mixed": "k_spmv_diff"}[precision]
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak_gbs, "unit": "GB/s",
             "frac": round(achieved / peak_gbs, 3), "traffic": None,
-            "kernel": f"{kern} (the SpMV of PCG step A, {precision})", "bytes_per_launch": int(nbytes),
+            "kernel": f"{kern} (the SpMV of PCG step A, {precision}, {lpg} lanes per node group)",
+            "bytes_per_launch": int(nbytes),
             "csr_formula_bytes": int(bytes_csr), "launch_us": round(t * 1e6, 2)}
 
 

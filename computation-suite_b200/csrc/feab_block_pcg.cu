@@ -1,0 +1,628 @@
+// Batched multi-RHS Jacobi-PCG: many independent problems (a block-diagonal K), each with a
+// panel of K right-hand sides, solved together.  Every RHS column runs its own CG recurrence
+// (its own alpha, beta, convergence test) -- the reference's preconditioned_cg
+// (iterative_solvers.py:434-481) applied column by column, as solve_static_batched
+// (batched_solve.py:105-164) applies one factorisation to many columns -- while the matrix is
+// read once per step for all columns of a problem (SpMM over the panel).
+//
+// Layout: vectors are row-major panels n x K (K = panel width, a power of two <= 64);
+// problem p owns a contiguous row range and a contiguous range of node row groups.  Work is
+// cut into items of <= 64 groups of one problem; a block processes items (grid-stride), and
+// reductions are per item then per problem: the last block to finish an item of problem p
+// (a per-problem ticket) reduces p's item partials in a fixed order, so results are
+// deterministic.  Converged problems are skipped; the host polls a "problems remaining"
+// counter one CUDA-graph chunk behind.
+//
+// Precisions: FEAB_PREC_FP64 (reference recurrence) and FEAB_PREC_MIXED (SpMM on 48-bit values
+// in difference form with FP64 vectors; per problem, an FP64 residual replacement with the
+// FP64 values whenever a column's residual dropped by reliable_delta; convergence on the FP64
+// residual).
+#include <algorithm>
+#include <cmath>
+#include "feab_common.cuh"
+
+namespace feab {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kWarps = kThreads / 32;
+constexpr int kModeCG = 0;
+constexpr int kModeReliable = 1;
+
+struct ProbState {  // per problem
+  int32_t mode, pending, psel, done, status, iters, reliable;
+  uint32_t ticket_a, ticket_b;
+};
+
+struct ColState {  // per (problem, column)
+  double bnorm, rz_old, rz_prev, alpha, beta, rr, relres, rmax;
+  int32_t active, iters, converged, pad;
+};
+
+struct BArgs {
+  int32_t n, n_groups, n_problems, n_items, k;
+  const int32_t* row_ptr;
+  const int32_t* col_idx;
+  const int32_t* group_ptr;
+  const double* vals64;
+  const uint32_t* vhi;
+  const uint16_t* vlo;
+  const int32_t* tcol;
+  const uint8_t* gmask;
+  const double* S;
+  const double* dinv;
+  const int32_t* item_problem;
+  const int32_t* item_g0;
+  const int32_t* item_g1;
+  const int32_t* prob_items;
+  const int32_t* prob_cols;
+  const double* B;   // n x k
+  double* X;         // n x k
+  double *R, *Z, *P0, *P1, *AP;
+  double* part;      // n_items x 2k
+  ProbState* ps;
+  ColState* cs;
+  int32_t* remaining;
+  double tol, delta;
+  int32_t maxiter;
+};
+
+__device__ __forceinline__ bool last_of_problem(uint32_t* ticket, int n_items_p) {
+  __shared__ bool last;
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == (uint32_t)(n_items_p - 1));
+  __syncthreads();
+  return last;
+}
+
+// Block-wide per-column sums: thread t contributes v to column t % K (blockDim multiple of K).
+template <int K>
+__device__ __forceinline__ void block_col_sums(double v, double* sm) {
+  sm[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = kThreads / 2; s >= K; s >>= 1) {
+    if (threadIdx.x < s) sm[threadIdx.x] += sm[threadIdx.x + s];
+    __syncthreads();
+  }
+}
+
+__device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
+}
+
+// SpMM for one row group: acc[row][.] for this lane's panel columns.
+// Lanes are split into MPW = max(1, 32/K) sub-warps, each walking every MPW-th matrix column;
+// a lane covers CPL = max(1, K/32) panel columns c = (lane % min(K,32)) + 32*q.
+template <int K, bool DIFF, typename PF>
+__device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF pf, double (&acc)[3][K >= 32 ? K / 32 : 1]) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int MPW = K >= 32 ? 1 : 32 / K;
+  constexpr int LW = K >= 32 ? 32 : K;  // lanes per sub-warp
+  const int sub = lane / LW, cl = lane % LW;
+  const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+  const int s0 = A.row_ptr[r0], len = A.row_ptr[r0 + 1] - s0;
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) acc[k][q] = 0.0;
+  double xs[3][CPL];
+  int mask = 0;
+  if (DIFF) {
+    mask = A.gmask[g];
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+#pragma unroll
+      for (int q = 0; q < CPL; ++q)
+        xs[j][q] = ((mask >> j) & 1) ? pf(r0 + __popc(mask & ((1 << j) - 1)), cl + 32 * q, q) : 0.0;
+  }
+  for (int m = sub; m < len; m += MPW) {
+    if (!DIFF) {
+      const int j = __ldg(A.col_idx + s0 + m);
+      double w[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) w[k] = k < f ? __ldg(A.vals64 + s0 + k * len + m) : 0.0;
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const double xv = pf(j, cl + 32 * q, q);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * xv;
+      }
+    } else {
+      const unsigned t = (unsigned)__ldg(A.tcol + s0 + m);
+      const int j = (int)(t & 0x3fffffffu), jc = (int)(t >> 30);
+      if (j >= r0 && j < r0 + f) continue;  // own node: K_aa (x_a - x_a) = 0
+      double w[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+        w[k] = k < f ? dec48(__ldg(A.vhi + s0 + k * len + m), __ldg(A.vlo + s0 + k * len + m)) : 0.0;
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const double d = pf(j, cl + 32 * q, q) - xs[jc][q];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * d;
+      }
+    }
+  }
+  // combine the sub-warps (lanes with equal cl)
+#pragma unroll
+  for (int o = LW; o < 32; o <<= 1)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) acc[k][q] += __shfl_xor_sync(FEAB_FULL_MASK, acc[k][q], o);
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k < f) {
+        const double s0v = A.S[(int64_t)(r0 + k) * 3 + 0], s1v = A.S[(int64_t)(r0 + k) * 3 + 1],
+                     s2v = A.S[(int64_t)(r0 + k) * 3 + 2];
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) acc[k][q] += s0v * xs[0][q] + s1v * xs[1][q] + s2v * xs[2][q];
+      }
+    }
+  }
+}
+
+// setup: R = B - 0 (x0 = 0), Z = M R, P = Z, per column ||b||, r.z; columns beyond the problem's
+// RHS count are inactive from the start.
+template <int K>
+__global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
+  __shared__ double sm[2][kThreads];
+  const int c = threadIdx.x % K;
+  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+    const int p = A.item_problem[it];
+    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
+    double bb = 0.0, rz = 0.0;
+    for (int64_t idx = (int64_t)r0 * K + threadIdx.x; idx < (int64_t)r1 * K; idx += kThreads) {
+      const int i = (int)(idx / K);
+      const double bi = A.B[idx];
+      const double zi = A.dinv[i] * bi;
+      A.R[idx] = bi;
+      A.Z[idx] = zi;
+      A.P0[idx] = zi;
+      A.X[idx] = 0.0;
+      bb += bi * bi;
+      rz += bi * zi;
+    }
+    block_col_sums<K>(bb, sm[0]);
+    block_col_sums<K>(rz, sm[1]);
+    if (threadIdx.x < K) {
+      A.part[(int64_t)it * 2 * K + c] = sm[0][c];
+      A.part[(int64_t)it * 2 * K + K + c] = sm[1][c];
+    }
+    const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
+    if (last_of_problem(&A.ps[p].ticket_a, n_it)) {
+      if (threadIdx.x < K) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int q = 0; q < n_it; ++q) {
+          s0 += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
+          s1 += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + K + c]);
+        }
+        ColState& C = A.cs[(int64_t)p * K + c];
+        double bn = sqrt(s0);
+        if (bn == 0.0) bn = 1.0;
+        C.bnorm = bn;
+        C.rz_old = s1;
+        C.rz_prev = s1;
+        C.rr = s0;
+        C.rmax = sqrt(s0);
+        C.relres = sqrt(s0) / bn;
+        C.alpha = C.beta = 0.0;
+        C.iters = 0;
+        C.active = c < A.prob_cols[p] ? 1 : 0;
+        C.converged = (!C.active || C.relres < A.tol) ? 1 : 0;
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        ProbState& P = A.ps[p];
+        int all = 1;
+        for (int q = 0; q < K; ++q) all &= A.cs[(int64_t)p * K + q].converged;
+        P.ticket_a = 0;
+        P.mode = kModeCG;
+        P.pending = 0;
+        P.psel = 0;
+        P.iters = 0;
+        P.reliable = 0;
+        P.status = FEAB_OK;
+        P.done = all;
+        if (all) atomicSub(A.remaining, 1);
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Step A: P_new = Z + beta P_old on the fly; AP = K P_new (or, in a reliable step, R = B - K64 X);
+// per-column partial p.Ap (or r.r).
+template <int K, bool MIXED>
+__global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int LW = K >= 32 ? 32 : K;
+  __shared__ double sm[kWarps][K];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+    const int p = A.item_problem[it];
+    const ProbState P = A.ps[p];
+    if (P.done) continue;
+    const bool reliable = MIXED && P.mode == kModeReliable;
+    const double* po = P.psel ? A.P1 : A.P0;
+    double* pn = P.psel ? A.P0 : A.P1;
+    const int pend = P.pending;
+    double beta[CPL];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) beta[q] = A.cs[(int64_t)p * K + (lane % LW) + 32 * q].beta;
+    double part[CPL];
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) part[q] = 0.0;
+    for (int g = A.item_g0[it] + w; g < A.item_g1[it]; g += kWarps) {
+      double acc[3][CPL];
+      if (reliable) {
+        group_spmm<K, false>(A, g, lane, [&](int j, int c, int) { return A.X[(int64_t)j * K + c]; }, acc);
+      } else if (pend) {
+        group_spmm<K, MIXED>(A, g, lane, [&](int j, int c, int q) {
+          return A.Z[(int64_t)j * K + c] + beta[q] * po[(int64_t)j * K + c]; }, acc);
+      } else {
+        group_spmm<K, MIXED>(A, g, lane, [&](int j, int c, int) { return po[(int64_t)j * K + c]; }, acc);
+      }
+      if (lane < LW) {
+        const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+        for (int k = 0; k < f; ++k) {
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const int64_t idx = (int64_t)(r0 + k) * K + lane + 32 * q;
+            if (reliable) {
+              const double ri = A.B[idx] - acc[k][q];
+              A.R[idx] = ri;
+              part[q] += ri * ri;
+            } else {
+              const double pv = pend ? A.Z[idx] + beta[q] * po[idx] : po[idx];
+              if (pend) pn[idx] = pv;
+              A.AP[idx] = acc[k][q];
+              part[q] += pv * acc[k][q];
+            }
+          }
+        }
+      }
+    }
+    if (lane < LW) {
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) sm[w][lane + 32 * q] = part[q];
+    }
+    __syncthreads();
+    if (threadIdx.x < K) {
+      double s = 0.0;
+      for (int q = 0; q < kWarps; ++q) s += sm[q][threadIdx.x];
+      A.part[(int64_t)it * 2 * K + threadIdx.x] = s;
+    }
+    const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
+    if (last_of_problem(&A.ps[p].ticket_a, n_it)) {
+      if (threadIdx.x < K) {
+        const int c = threadIdx.x;
+        double s = 0.0;
+        for (int q = 0; q < n_it; ++q) s += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
+        ColState& C = A.cs[(int64_t)p * K + c];
+        if (reliable) {
+          C.rr = s;
+        } else {
+          C.alpha = 0.0;
+          if (C.active && !C.converged) {
+            if (!(s > 0.0)) atomicCAS(&A.ps[p].status, FEAB_OK, FEAB_NOT_SPD);
+            else C.alpha = C.rz_old / s;
+          }
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        ProbState& Pm = A.ps[p];
+        Pm.ticket_a = 0;
+        if (!reliable) {
+          if (pend) Pm.psel ^= 1;
+          Pm.pending = 0;
+          if (Pm.status != FEAB_OK) {
+            Pm.done = 1;
+            atomicSub(A.remaining, 1);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+// Step B: X += alpha P, R -= alpha AP, Z = M R (CG) or Z = M R (reliable); per column r.r, r.z;
+// per-column convergence, beta, problem bookkeeping.
+template <int K, bool MIXED>
+__global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
+  __shared__ double sm[2][kThreads];
+  __shared__ int flag_reliable;
+  const int c = threadIdx.x % K;
+  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+    const int p = A.item_problem[it];
+    const ProbState P = A.ps[p];
+    if (P.done) continue;
+    const bool reliable = MIXED && P.mode == kModeReliable;
+    const double alpha = A.cs[(int64_t)p * K + c].alpha;
+    const double* pc = P.psel ? A.P1 : A.P0;
+    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
+    double rr = 0.0, rz = 0.0;
+    for (int64_t idx = (int64_t)r0 * K + threadIdx.x; idx < (int64_t)r1 * K; idx += kThreads) {
+      const int i = (int)(idx / K);
+      double ri;
+      if (reliable) {
+        ri = A.R[idx];
+      } else {
+        A.X[idx] += alpha * pc[idx];
+        ri = A.R[idx] - alpha * A.AP[idx];
+        A.R[idx] = ri;
+      }
+      const double zi = A.dinv[i] * ri;
+      A.Z[idx] = zi;
+      rr += ri * ri;
+      rz += ri * zi;
+    }
+    block_col_sums<K>(rr, sm[0]);
+    block_col_sums<K>(rz, sm[1]);
+    if (threadIdx.x < K) {
+      A.part[(int64_t)it * 2 * K + c] = sm[0][c];
+      A.part[(int64_t)it * 2 * K + K + c] = sm[1][c];
+    }
+    const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
+    if (last_of_problem(&A.ps[p].ticket_b, n_it)) {
+      if (threadIdx.x == 0) flag_reliable = 0;
+      __syncthreads();
+      if (threadIdx.x < K) {
+        double s0 = 0.0, s1 = 0.0;
+        for (int q = 0; q < n_it; ++q) {
+          s0 += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
+          s1 += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + K + c]);
+        }
+        ColState& C = A.cs[(int64_t)p * K + c];
+        if (C.active && !C.converged) {
+          if (!reliable) C.iters += 1;
+          const double rrv = reliable ? C.rr : s0;
+          const double rel = sqrt(rrv) / C.bnorm;
+          C.relres = rel;
+          const bool conv = rel < A.tol;
+          if (!MIXED || reliable) {
+            if (conv) C.converged = 1;
+            if (reliable) C.rmax = sqrt(rrv);
+          } else if (conv || sqrt(rrv) < A.delta * C.rmax) {
+            atomicOr(&flag_reliable, 1);
+          }
+          if (reliable) {
+            C.beta = s1 / C.rz_prev;  // r replaced the recurrence residual of the previous step
+          } else {
+            C.rz_prev = C.rz_old;
+            C.beta = s1 / C.rz_old;
+          }
+          C.rz_old = s1;
+        }
+        if (!C.active || C.converged) C.beta = 0.0;  // frozen columns: p = z, alpha = 0
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        ProbState& Pm = A.ps[p];
+        Pm.ticket_b = 0;
+        if (!reliable) Pm.iters += 1;
+        else Pm.reliable += 1;
+        int all = 1;
+        for (int q = 0; q < K; ++q) all &= A.cs[(int64_t)p * K + q].converged;
+        if (MIXED && !reliable && flag_reliable) {
+          // FP64 residual replacement next; the search directions wait for it.  rz_old of the
+          // columns was advanced above; it is recomputed from the replaced residual.
+          Pm.mode = kModeReliable;
+          Pm.pending = 0;
+        } else {
+          Pm.mode = kModeCG;
+          Pm.pending = 1;
+        }
+        if (all) {
+          Pm.done = 1;
+          atomicSub(A.remaining, 1);
+        } else if (Pm.iters >= A.maxiter) {
+          Pm.done = 1;
+          Pm.status = FEAB_NOT_CONVERGED;
+          atomicSub(A.remaining, 1);
+        }
+      }
+    }
+    __syncthreads();
+  }
+}
+
+size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
+
+struct BLayout {
+  size_t total;
+  size_t o_R, o_Z, o_P0, o_P1, o_AP, o_part, o_ps, o_cs, o_rem;
+};
+
+BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
+  BLayout L{};
+  size_t off = 0;
+  auto take = [&](size_t b) {
+    size_t o = off;
+    off += a256(b);
+    return o;
+  };
+  const size_t panel = sizeof(double) * (size_t)n * (size_t)k;
+  L.o_R = take(panel);
+  L.o_Z = take(panel);
+  L.o_P0 = take(panel);
+  L.o_P1 = take(panel);
+  L.o_AP = take(panel);
+  L.o_part = take(sizeof(double) * 2 * (size_t)k * (size_t)n_items);
+  L.o_ps = take(sizeof(ProbState) * (size_t)n_problems);
+  L.o_cs = take(sizeof(ColState) * (size_t)n_problems * (size_t)k);
+  L.o_rem = take(sizeof(int32_t));
+  L.total = off;
+  return L;
+}
+
+template <int K>
+int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int32_t* host_iters, double* host_relres,
+                  int32_t* host_status) {
+  const int grid = std::max(1, std::min(A.n_items, sm_count() * 4));
+  cudaMemsetAsync(A.ps, 0, sizeof(ProbState) * A.n_problems, s);
+  int32_t np = A.n_problems;
+  cudaMemcpyAsync(A.remaining, &np, sizeof(int32_t), cudaMemcpyHostToDevice, s);
+  k_bsetup<K><<<grid, kThreads, 0, s>>>(A);
+  count_launches(1);
+  if (cudaGetLastError() != cudaSuccess) return FEAB_CUDA_ERROR;
+  int32_t* hflag = nullptr;
+  if (cudaHostAlloc((void**)&hflag, 64, cudaHostAllocDefault) != cudaSuccess) return FEAB_CUDA_ERROR;
+  cudaStream_t cs = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaEvent_t ev[2] = {nullptr, nullptr};
+  int32_t rc = FEAB_OK;
+  auto fail = [&](cudaError_t e) {
+    if (e != cudaSuccess && rc == FEAB_OK) rc = FEAB_CUDA_ERROR;
+    return e != cudaSuccess;
+  };
+  do {
+    if (fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking))) break;
+    if (fail(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming))) break;
+    if (fail(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) break;
+    if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
+    for (int q = 0; q < chunk; ++q) {
+      if (prec == FEAB_PREC_MIXED) {
+        k_bstep_a<K, true><<<grid, kThreads, 0, cs>>>(A);
+        k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
+      } else {
+        k_bstep_a<K, false><<<grid, kThreads, 0, cs>>>(A);
+        k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
+      }
+    }
+    cudaMemcpyAsync(hflag, A.remaining, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
+    if (fail(cudaStreamEndCapture(cs, &graph))) break;
+    if (fail(cudaGraphInstantiate(&exec, graph, 0))) break;
+    // iterations and reliable steps per problem are bounded by maxiter each
+    const int64_t max_launch = (2 * (int64_t)maxiter + 2 + chunk - 1) / chunk + 1;
+    hflag[0] = np;
+    int64_t launched = 0;
+    if (fail(cudaGraphLaunch(exec, s))) break;
+    if (fail(cudaEventRecord(ev[0], s))) break;
+    launched = 1;
+    count_launches(2 * (uint64_t)chunk);
+    while (true) {
+      const bool more = launched < max_launch;
+      if (more) {
+        if (fail(cudaGraphLaunch(exec, s))) break;
+        if (fail(cudaEventRecord(ev[launched & 1], s))) break;
+        ++launched;
+        count_launches(2 * (uint64_t)chunk);
+      }
+      if (fail(cudaEventSynchronize(ev[more ? ((launched - 2) & 1) : ((launched - 1) & 1)]))) break;
+      if (((volatile int32_t*)hflag)[0] <= 0 || !more) break;
+    }
+  } while (false);
+  if (rc == FEAB_OK) fail(cudaStreamSynchronize(s));
+  int32_t worst = rc;
+  if (rc == FEAB_OK) {
+    // per-problem / per-column results
+    const int P = A.n_problems;
+    ProbState* hp = (ProbState*)malloc(sizeof(ProbState) * P);
+    ColState* hc = (ColState*)malloc(sizeof(ColState) * (size_t)P * K);
+    if (hp && hc && cudaMemcpy(hp, A.ps, sizeof(ProbState) * P, cudaMemcpyDeviceToHost) == cudaSuccess &&
+        cudaMemcpy(hc, A.cs, sizeof(ColState) * (size_t)P * K, cudaMemcpyDeviceToHost) == cudaSuccess) {
+      for (int p = 0; p < P; ++p) {
+        int st = hp[p].status;
+        if (!hp[p].done) st = FEAB_NOT_CONVERGED;
+        if (host_status) host_status[p] = st;
+        if (st != FEAB_OK && worst == FEAB_OK) worst = st;
+        for (int c = 0; c < K; ++c) {
+          if (host_iters) host_iters[(size_t)p * K + c] = hc[(size_t)p * K + c].iters;
+          if (host_relres) host_relres[(size_t)p * K + c] = hc[(size_t)p * K + c].relres;
+        }
+      }
+    } else {
+      worst = FEAB_CUDA_ERROR;
+    }
+    free(hp);
+    free(hc);
+  }
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (ev[0]) cudaEventDestroy(ev[0]);
+  if (ev[1]) cudaEventDestroy(ev[1]);
+  if (cs) cudaStreamDestroy(cs);
+  cudaFreeHost(hflag);
+  return worst;
+}
+
+}  // namespace
+}  // namespace feab
+
+using namespace feab;
+
+extern "C" size_t feab_block_pcg_workspace_bytes(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
+  if (n <= 0 || k <= 0 || n_problems <= 0 || n_items <= 0) return 0;
+  return blayout(n, k, n_problems, n_items).total;
+}
+
+extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_operator* D, const feab_batch* bt,
+                                        const double* dinv64, const double* B, double* X, const feab_pcg_params* prm,
+                                        void* workspace, size_t workspace_bytes, int32_t* iters_out,
+                                        double* relres_out, int32_t* status_out, cudaStream_t s) {
+  if (!M || !bt || !dinv64 || !B || !X || !prm || !workspace || !M->group_ptr || !M->vals64) return FEAB_BAD_ARG;
+  const int k = bt->k;
+  if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64) return FEAB_BAD_ARG;
+  if (bt->n_problems <= 0 || bt->n_items <= 0 || !bt->item_problem || !bt->item_group0 || !bt->item_group1 ||
+      !bt->problem_items || !bt->problem_cols)
+    return FEAB_BAD_ARG;
+  const int prec = prm->precision;
+  if (prec != FEAB_PREC_FP64 && prec != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
+  if (prec == FEAB_PREC_MIXED && !D) return FEAB_BAD_ARG;
+  const BLayout L = blayout(M->n, k, bt->n_problems, bt->n_items);
+  if (L.total > workspace_bytes) return FEAB_BAD_ARG;
+  char* w = static_cast<char*>(workspace);
+  BArgs A{};
+  A.n = M->n;
+  A.n_groups = M->n_groups;
+  A.n_problems = bt->n_problems;
+  A.n_items = bt->n_items;
+  A.k = k;
+  A.row_ptr = M->row_ptr;
+  A.col_idx = M->col_idx;
+  A.group_ptr = M->group_ptr;
+  A.vals64 = M->vals64;
+  if (D) {
+    A.vhi = D->vhi;
+    A.vlo = D->vlo;
+    A.tcol = D->tcol;
+    A.gmask = D->gmask;
+    A.S = D->S;
+  }
+  A.dinv = dinv64;
+  A.item_problem = bt->item_problem;
+  A.item_g0 = bt->item_group0;
+  A.item_g1 = bt->item_group1;
+  A.prob_items = bt->problem_items;
+  A.prob_cols = bt->problem_cols;
+  A.B = B;
+  A.X = X;
+  A.R = reinterpret_cast<double*>(w + L.o_R);
+  A.Z = reinterpret_cast<double*>(w + L.o_Z);
+  A.P0 = reinterpret_cast<double*>(w + L.o_P0);
+  A.P1 = reinterpret_cast<double*>(w + L.o_P1);
+  A.AP = reinterpret_cast<double*>(w + L.o_AP);
+  A.part = reinterpret_cast<double*>(w + L.o_part);
+  A.ps = reinterpret_cast<ProbState*>(w + L.o_ps);
+  A.cs = reinterpret_cast<ColState*>(w + L.o_cs);
+  A.remaining = reinterpret_cast<int32_t*>(w + L.o_rem);
+  A.tol = prm->tol;
+  A.delta = prm->reliable_delta > 0.0 && prm->reliable_delta < 1.0 ? prm->reliable_delta : 0.1;
+  A.maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
+  const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
+  switch (k) {
+    case 1: return run_block<1>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    case 2: return run_block<2>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    case 4: return run_block<4>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    case 8: return run_block<8>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    case 16: return run_block<16>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    case 32: return run_block<32>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+    default: return run_block<64>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
+  }
+}

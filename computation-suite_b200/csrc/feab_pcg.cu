@@ -110,43 +110,96 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, u
   return true;
 }
 
-__device__ __forceinline__ void group_rows(const PcgArgs& A, int g, int& r0, int& f) {
-  if (A.group_ptr) {
-    r0 = A.group_ptr[g];
-    f = A.group_ptr[g + 1] - r0;
-  } else {
-    r0 = g;
-    f = 1;
+// A row group's rows (r0 .. r0+f-1), the first row's start in col_idx / vals, and its length
+// (all rows of a group have the same length and sit back to back in vals).
+struct Group {
+  int g, r0, f, s0, len, mask;
+  bool valid;
+};
+
+// Visits every row group.  Each warp owns tiles of 32 consecutive groups; lane l loads the
+// descriptor of the tile's l-th group (group_ptr -> row_ptr, plus the free-DOF mask when
+// `with_mask`), so the two dependent pointer loads are paid once per 32 groups.  The warp is
+// split into 32/LPG sub-warps of LPG lanes; sub-warp s takes groups s, s + 32/LPG, ... of the
+// tile, so 32/LPG groups have their loads in flight at once.  Lanes of a sub-warp with no group
+// left get len = 0 (they still join the sub-warp's shuffles) and `valid` false.
+template <int LPG, bool with_mask, typename F>
+__device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn) {
+  constexpr int NSG = 32 / LPG;
+  const int G = A.group_ptr ? A.n_groups : A.n;
+  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
+  const int ntiles = (G + 31) >> 5;
+  const int sg = lane / LPG;
+  for (int tile = wg; tile < ntiles; tile += nw) {
+    const int g = (tile << 5) + lane;
+    int r0 = 0, f = 0, s0 = 0, len = 0, mask = 0;
+    if (g < G) {
+      if (A.group_ptr) {
+        r0 = __ldg(A.group_ptr + g);
+        f = __ldg(A.group_ptr + g + 1) - r0;
+      } else {
+        r0 = g;
+        f = 1;
+      }
+      s0 = __ldg(A.row_ptr + r0);
+      len = __ldg(A.row_ptr + r0 + 1) - s0;
+      if (with_mask) mask = A.gmask[g];
+    }
+    const int cnt = min(32, G - (tile << 5));
+    for (int i = 0; i < cnt; i += NSG) {
+      const int src = (i + sg) & 31;
+      Group gr;
+      gr.g = (tile << 5) + i + sg;
+      gr.r0 = __shfl_sync(FEAB_FULL_MASK, r0, src);
+      gr.f = __shfl_sync(FEAB_FULL_MASK, f, src);
+      gr.s0 = __shfl_sync(FEAB_FULL_MASK, s0, src);
+      gr.len = __shfl_sync(FEAB_FULL_MASK, len, src);
+      gr.mask = with_mask ? __shfl_sync(FEAB_FULL_MASK, mask, src) : 0;
+      gr.valid = i + sg < cnt;
+      if (!gr.valid) {
+        gr.f = 0;
+        gr.len = 0;
+      }
+      fn(gr);
+    }
   }
 }
 
-// acc[k] = sum_c vals[row r0+k, c] * xf(col c) for the f (<= 3) rows of a group.
-template <typename AT, typename VT, typename XF>
-__device__ __forceinline__ void group_spmv(const PcgArgs& A, const VT* __restrict__ vals, int r0, int f, int lane,
+// Sum over the LPG lanes of a sub-warp (xor offsets below LPG stay inside the sub-warp).
+template <int LPG, typename T>
+__device__ __forceinline__ T seg_sum(T v) {
+#pragma unroll
+  for (int o = LPG / 2; o > 0; o >>= 1) v += __shfl_xor_sync(FEAB_FULL_MASK, v, o);
+  return v;
+}
+
+// acc[k] = sum_c vals[row r0+k, c] * xf(col c) for the f (<= 3) rows of a group, over the
+// group's LPG lanes (hl = lane within the sub-warp), 3 column passes issued together.
+template <int LPG, typename AT, typename VT, typename XF>
+__device__ __forceinline__ void group_spmv(const PcgArgs& A, const VT* __restrict__ vals, const Group& G, int hl,
                                            XF xf, AT (&acc)[3]) {
-  const int s0 = A.row_ptr[r0];
-  const int len = A.row_ptr[r0 + 1] - s0;
-  const int32_t* __restrict__ col = A.col_idx + s0;
-  const VT* __restrict__ v0 = vals + s0;
+  const int len = G.len, f = G.f;
+  const int32_t* __restrict__ col = A.col_idx + G.s0;
+  const VT* __restrict__ v0 = vals + G.s0;
   AT a0 = 0, a1 = 0, a2 = 0;
-  for (int c = lane; c < len; c += 96) {
-    const bool p1 = c + 32 < len, p2 = c + 64 < len;
+  for (int c = hl; c < len; c += 3 * LPG) {
+    const bool p1 = c + LPG < len, p2 = c + 2 * LPG < len;
     const int j0 = __ldg(col + c);
-    const int j1 = p1 ? __ldg(col + c + 32) : 0;
-    const int j2 = p2 ? __ldg(col + c + 64) : 0;
+    const int j1 = p1 ? __ldg(col + c + LPG) : 0;
+    const int j2 = p2 ? __ldg(col + c + 2 * LPG) : 0;
     const AT w00 = (AT)__ldg(v0 + c);
-    const AT w01 = p1 ? (AT)__ldg(v0 + c + 32) : AT(0);
-    const AT w02 = p2 ? (AT)__ldg(v0 + c + 64) : AT(0);
+    const AT w01 = p1 ? (AT)__ldg(v0 + c + LPG) : AT(0);
+    const AT w02 = p2 ? (AT)__ldg(v0 + c + 2 * LPG) : AT(0);
     AT w10 = 0, w11 = 0, w12 = 0, w20 = 0, w21 = 0, w22 = 0;
     if (f > 1) {
       w10 = (AT)__ldg(v0 + len + c);
-      w11 = p1 ? (AT)__ldg(v0 + len + c + 32) : AT(0);
-      w12 = p2 ? (AT)__ldg(v0 + len + c + 64) : AT(0);
+      w11 = p1 ? (AT)__ldg(v0 + len + c + LPG) : AT(0);
+      w12 = p2 ? (AT)__ldg(v0 + len + c + 2 * LPG) : AT(0);
     }
     if (f > 2) {
       w20 = (AT)__ldg(v0 + 2 * len + c);
-      w21 = p1 ? (AT)__ldg(v0 + 2 * len + c + 32) : AT(0);
-      w22 = p2 ? (AT)__ldg(v0 + 2 * len + c + 64) : AT(0);
+      w21 = p1 ? (AT)__ldg(v0 + 2 * len + c + LPG) : AT(0);
+      w22 = p2 ? (AT)__ldg(v0 + 2 * len + c + 2 * LPG) : AT(0);
     }
     const AT x0 = xf(j0);
     const AT x1 = p1 ? xf(j1) : AT(0);
@@ -155,9 +208,9 @@ __device__ __forceinline__ void group_spmv(const PcgArgs& A, const VT* __restric
     a1 += w10 * x0 + w11 * x1 + w12 * x2;
     a2 += w20 * x0 + w21 * x1 + w22 * x2;
   }
-  acc[0] = warp_sum(a0);
-  acc[1] = f > 1 ? warp_sum(a1) : AT(0);
-  acc[2] = f > 2 ? warp_sum(a2) : AT(0);
+  acc[0] = seg_sum<LPG>(a0);
+  acc[1] = seg_sum<LPG>(a1);
+  acc[2] = seg_sum<LPG>(a2);
 }
 
 __device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
@@ -166,44 +219,54 @@ __device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
 
 // Difference-form SpMV over one group with 48-bit values:
 // acc[k] = sum_{c, col(c) not in own node} v[c] (x(col c) - xs[j(c)]) + sum_j S[r0+k][j] xs[j].
-template <typename XF>
-__device__ __forceinline__ void group_spmv_diff(const PcgArgs& A, int g, int r0, int f, int lane, XF xf,
-                                                double (&acc)[3]) {
-  const int mask = A.gmask[g];
+// Values are loaded for every column (own-node columns are multiplied by zero) so that the
+// value loads do not wait for the column loads.
+template <int LPG, typename XF>
+__device__ __forceinline__ void group_spmv_diff(const PcgArgs& A, const Group& G, int hl, XF xf, double (&acc)[3]) {
+  const int r0 = G.r0, f = G.f, len = G.len, mask = G.mask;
+  const int32_t* __restrict__ col = A.tcol + G.s0;
+  const uint32_t* __restrict__ hi = A.vhi + G.s0;
+  const uint16_t* __restrict__ lo = A.vlo + G.s0;
   double xs[3];
 #pragma unroll
-  for (int j = 0; j < 3; ++j) xs[j] = ((mask >> j) & 1) ? xf(r0 + __popc(mask & ((1 << j) - 1))) : 0.0;
-  const int s0 = A.row_ptr[r0];
-  const int len = A.row_ptr[r0 + 1] - s0;
-  const int32_t* __restrict__ col = A.tcol + s0;
-  double a[3] = {0.0, 0.0, 0.0};
-  for (int c0 = lane; c0 < len; c0 += 96) {
-    int jj[3];
-    double d[3];
+  for (int j = 0; j < 3; ++j) xs[j] = (G.valid && ((mask >> j) & 1)) ? xf(r0 + __popc(mask & ((1 << j) - 1))) : 0.0;
+  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+  for (int c0 = hl; c0 < len; c0 += 3 * LPG) {
+    unsigned t[3];
+    uint32_t h[3][3];
+    uint16_t l[3][3];
 #pragma unroll
     for (int u = 0; u < 3; ++u) {
-      const int c = c0 + 32 * u;
-      const unsigned t = c < len ? (unsigned)__ldg(col + c) : 0u;
-      const int cj = (int)(t & 0x3fffffffu);
-      const bool own = c >= len || (cj >= r0 && cj < r0 + f);
-      jj[u] = own ? -1 : c;
-      d[u] = own ? 0.0 : xf(cj) - xs[t >> 30];
-    }
+      const int c = c0 + LPG * u;
+      const bool ok = c < len;
+      t[u] = ok ? (unsigned)__ldg(col + c) : 0u;
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      if (k < f) {
-        const int off = s0 + k * len;
-#pragma unroll
-        for (int u = 0; u < 3; ++u)
-          if (jj[u] >= 0) a[k] += dec48(__ldg(A.vhi + off + jj[u]), __ldg(A.vlo + off + jj[u])) * d[u];
+      for (int k = 0; k < 3; ++k) {
+        const bool okk = ok && k < f;
+        h[k][u] = okk ? __ldg(hi + k * len + c) : 0u;
+        l[k][u] = okk ? __ldg(lo + k * len + c) : (uint16_t)0;
       }
     }
-  }
 #pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    acc[k] = k < f ? warp_sum(a[k]) : 0.0;
-    if (k < f) acc[k] += A.S[(r0 + k) * 3 + 0] * xs[0] + A.S[(r0 + k) * 3 + 1] * xs[1] + A.S[(r0 + k) * 3 + 2] * xs[2];
+    for (int u = 0; u < 3; ++u) {
+      const int c = c0 + LPG * u;
+      const int cj = (int)(t[u] & 0x3fffffffu);
+      const bool own = c >= len || (cj >= r0 && cj < r0 + f);
+      const double d = own ? 0.0 : xf(cj) - xs[t[u] >> 30];
+      a0 += dec48(h[0][u], l[0][u]) * d;
+      a1 += dec48(h[1][u], l[1][u]) * d;
+      a2 += dec48(h[2][u], l[2][u]) * d;
+    }
   }
+  // S[r0+k][j] row-block sums (own-node part of the difference form)
+  const double* __restrict__ Sp = A.S + (int64_t)r0 * 3;
+  double sx[3];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+    sx[k] = k < f ? __ldg(Sp + 3 * k) * xs[0] + __ldg(Sp + 3 * k + 1) * xs[1] + __ldg(Sp + 3 * k + 2) * xs[2] : 0.0;
+  acc[0] = seg_sum<LPG>(a0) + sx[0];
+  acc[1] = seg_sum<LPG>(a1) + sx[1];
+  acc[2] = seg_sum<LPG>(a2) + sx[2];
 }
 
 __device__ __forceinline__ double pick3(const double (&a)[3], int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
@@ -228,27 +291,24 @@ __global__ void k_init_state(PcgState* S, double tol, double delta, int maxiter)
 
 // r = b - K64 x0 (plain form, FP64); ||b||, ||r||; early exit as iterative_solvers.py:437-443.
 // fp32 mode writes the FP64 residual to r64, the others to r.
-template <int PREC>
+template <int PREC, int LPG>
 __global__ void __launch_bounds__(kThreads) k_setup_a(PcgArgs A) {
   PcgState* S = A.S_;
   const int lane = threadIdx.x & 31;
-  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  const int G = A.group_ptr ? A.n_groups : A.n;
+  const int hl = lane % LPG;
   double* r = PREC == FEAB_PREC_FP32 ? A.r64 : A.r;
   double part[2] = {0.0, 0.0};
-  for (int g = wg; g < G; g += nw) {
-    int r0, f;
-    group_rows(A, g, r0, f);
+  for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
     double acc[3] = {0.0, 0.0, 0.0};
-    if (A.x0) group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.x0 + j); }, acc);
-    if (lane < f) {
-      const double bi = A.b[r0 + lane];
-      const double ri = bi - pick3(acc, lane);
-      r[r0 + lane] = ri;
+    if (A.x0) group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.x0 + j); }, acc);
+    if (hl < gr.f) {
+      const double bi = A.b[gr.r0 + hl];
+      const double ri = bi - pick3(acc, hl);
+      r[gr.r0 + hl] = ri;
       part[0] += bi * bi;
       part[1] += ri * ri;
     }
-  }
+  });
   double tot[2];
   if (grid_reduce<2>(part, A.partials, &S->ticket[0], tot) && threadIdx.x == 0) {
     double bn = sqrt(tot[0]);
@@ -298,101 +358,92 @@ __global__ void __launch_bounds__(kThreads) k_setup_b(PcgArgs A) {
 }
 
 // Step kernel A.
-template <int PREC>
-__global__ void __launch_bounds__(kThreads) k_step_a(PcgArgs A) {
+template <int PREC, int LPG>
+__global__ void __launch_bounds__(kThreads, 4) k_step_a(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
   const int pend = S->p_pending;
   const int psel = S->psel;
   const int lane = threadIdx.x & 31;
-  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  const int G = A.group_ptr ? A.n_groups : A.n;
+  const int hl = lane % LPG;
   double part[1] = {0.0};
   if (PREC == FEAB_PREC_FP32 && mode == kModeReliable) {
     // r64 = b - K64 (x64 + x32); x64' = x64 + x32 (other half of the ping-pong)
     const double* xin = S->xsel ? A.x64b : A.x64a;
     double* xout = S->xsel ? A.x64a : A.x64b;
-    for (int g = wg; g < G; g += nw) {
-      int r0, f;
-      group_rows(A, g, r0, f);
+    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
       double acc[3];
-      group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(xin + j) + (double)__ldg(A.x32 + j); },
+      group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(xin + j) + (double)__ldg(A.x32 + j); },
                          acc);
-      if (lane < f) {
-        const int i = r0 + lane;
-        const double ri = A.b[i] - pick3(acc, lane);
+      if (hl < gr.f) {
+        const int i = gr.r0 + hl;
+        const double ri = A.b[i] - pick3(acc, hl);
         A.r64[i] = ri;
         xout[i] = xin[i] + (double)A.x32[i];
         part[0] += ri * ri;
       }
-    }
+    });
   } else if (PREC == FEAB_PREC_MIXED && mode == kModeReliable) {
     // FP64 residual with the exact FP64 values: r = b - K64 x
-    for (int g = wg; g < G; g += nw) {
-      int r0, f;
-      group_rows(A, g, r0, f);
+    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
       double acc[3];
-      group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.x + j); }, acc);
-      if (lane < f) {
-        const int i = r0 + lane;
-        const double ri = A.b[i] - pick3(acc, lane);
+      group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.x + j); }, acc);
+      if (hl < gr.f) {
+        const int i = gr.r0 + hl;
+        const double ri = A.b[i] - pick3(acc, hl);
         A.r[i] = ri;
         part[0] += ri * ri;
       }
-    }
+    });
   } else if (PREC == FEAB_PREC_FP32) {
     const float beta = (float)S->beta;
     const float* __restrict__ qo = psel ? A.q1 : A.q0;
     float* __restrict__ qn = psel ? A.q0 : A.q1;
-    for (int g = wg; g < G; g += nw) {
-      int r0, f;
-      group_rows(A, g, r0, f);
+    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
       float acc[3];
       if (pend) {
-        group_spmv<float>(A, A.vals32, r0, f, lane,
-                          [&](int j) { return fmaf(beta, __ldg(qo + j), __ldg(A.z32 + j)); }, acc);
+        group_spmv<LPG, float>(A, A.vals32, gr, hl, [&](int j) { return fmaf(beta, __ldg(qo + j), __ldg(A.z32 + j)); },
+                          acc);
       } else {
-        group_spmv<float>(A, A.vals32, r0, f, lane, [&](int j) { return __ldg(qo + j); }, acc);
+        group_spmv<LPG, float>(A, A.vals32, gr, hl, [&](int j) { return __ldg(qo + j); }, acc);
       }
-      if (lane < f) {
-        const int i = r0 + lane;
+      if (hl < gr.f) {
+        const int i = gr.r0 + hl;
         const float pi = pend ? fmaf(beta, qo[i], A.z32[i]) : qo[i];
         if (pend) qn[i] = pi;
-        const float v = pick3(acc, lane);
+        const float v = pick3(acc, hl);
         A.Ap32[i] = v;
         part[0] += (double)pi * (double)v;
       }
-    }
+    });
   } else {
     const double beta = S->beta;
     const double* __restrict__ po = psel ? A.p1 : A.p0;
     double* __restrict__ pn = psel ? A.p0 : A.p1;
-    for (int g = wg; g < G; g += nw) {
-      int r0, f;
-      group_rows(A, g, r0, f);
+    for_each_group<LPG, PREC == FEAB_PREC_MIXED>(A, lane, [&](const Group& gr) {
       double acc[3];
       if (PREC == FEAB_PREC_MIXED) {
         if (pend)
-          group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc);
+          group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc);
         else
-          group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(po + j); }, acc);
+          group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(po + j); }, acc);
       } else {
         if (pend)
-          group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); },
+          group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); },
                              acc);
         else
-          group_spmv<double>(A, A.vals64, r0, f, lane, [&](int j) { return __ldg(po + j); }, acc);
+          group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(po + j); }, acc);
       }
-      if (lane < f) {
-        const int i = r0 + lane;
+      if (hl < gr.f) {
+        const int i = gr.r0 + hl;
         const double pi = pend ? A.z[i] + beta * po[i] : po[i];
         if (pend) pn[i] = pi;
-        const double v = pick3(acc, lane);
+        const double v = pick3(acc, hl);
         A.Ap[i] = v;
         part[0] += pi * v;
       }
-    }
+    });
   }
   double tot[1];
   if (grid_reduce<1>(part, A.partials, &S->ticket[0], tot) && threadIdx.x == 0) {
@@ -518,33 +569,29 @@ __global__ void k_finalize_fp32(PcgArgs A) {
 }
 
 // Standalone y = A x with the step-A SpMV (same group_spmv code and launch shape).
-template <typename T>
-__global__ void __launch_bounds__(kThreads) k_spmv(PcgArgs A, const T* __restrict__ x, T* __restrict__ y) {
+template <typename T, int LPG>
+__global__ void __launch_bounds__(kThreads, 4) k_spmv(PcgArgs A, const T* __restrict__ x, T* __restrict__ y) {
   const int lane = threadIdx.x & 31;
-  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  const int G = A.group_ptr ? A.n_groups : A.n;
+  const int hl = lane % LPG;
   const T* vals;
   if constexpr (sizeof(T) == 8) vals = reinterpret_cast<const T*>(A.vals64);
   else vals = reinterpret_cast<const T*>(A.vals32);
-  for (int g = wg; g < G; g += nw) {
-    int r0, f;
-    group_rows(A, g, r0, f);
+  for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
     T acc[3];
-    group_spmv<T>(A, vals, r0, f, lane, [&](int j) { return __ldg(x + j); }, acc);
-    if (lane < f) y[r0 + lane] = pick3(acc, lane);
-  }
+    group_spmv<LPG, T>(A, vals, gr, hl, [&](int j) { return __ldg(x + j); }, acc);
+    if (hl < gr.f) y[gr.r0 + hl] = pick3(acc, hl);
+  });
 }
 
-__global__ void __launch_bounds__(kThreads) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
+template <int LPG>
+__global__ void __launch_bounds__(kThreads, 4) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
-  const int wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, nw = (gridDim.x * blockDim.x) >> 5;
-  for (int g = wg; g < A.n_groups; g += nw) {
-    int r0, f;
-    group_rows(A, g, r0, f);
+  const int hl = lane % LPG;
+  for_each_group<LPG, true>(A, lane, [&](const Group& gr) {
     double acc[3];
-    group_spmv_diff(A, g, r0, f, lane, [&](int j) { return __ldg(x + j); }, acc);
-    if (lane < f) y[r0 + lane] = pick3(acc, lane);
-  }
+    group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(x + j); }, acc);
+    if (hl < gr.f) y[gr.r0 + hl] = pick3(acc, hl);
+  });
 }
 
 // Difference-form operator from the FP64 CSR: tagged columns, 48-bit values, group masks and
@@ -603,7 +650,8 @@ struct Grids {
 
 Grids grids_for(int n, int G) {
   Grids g;
-  g.a = std::max(1, (int)std::min<int64_t>(((int64_t)G + 7) / 8, (int64_t)max_grid()));
+  // A: one warp per tile of 32 groups, 8 warps per block
+  g.a = std::max(1, (int)std::min<int64_t>(((int64_t)G + 255) / 256, (int64_t)max_grid()));
   g.b = std::max(1, (int)std::min<int64_t>(((int64_t)n + kThreads * 4 - 1) / (kThreads * 4), (int64_t)max_grid()));
   return g;
 }
@@ -672,25 +720,32 @@ struct HostFlag {
 };
 
 template <int PREC>
-void launch_setup(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
-  k_setup_a<PREC><<<gr.a, kThreads, 0, s>>>(A);
+void launch_setup(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
+  if (lpg == 8) k_setup_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
+  else if (lpg == 16) k_setup_a<PREC, 16><<<gr.a, kThreads, 0, s>>>(A);
+  else k_setup_a<PREC, 32><<<gr.a, kThreads, 0, s>>>(A);
   k_setup_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
   count_launches(2);
 }
 
 template <int PREC>
-void launch_step(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
-  k_step_a<PREC><<<gr.a, kThreads, 0, s>>>(A);
+void launch_step(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
+  if (lpg == 8) k_step_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
+  else if (lpg == 16) k_step_a<PREC, 16><<<gr.a, kThreads, 0, s>>>(A);
+  else k_step_a<PREC, 32><<<gr.a, kThreads, 0, s>>>(A);
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
 }
 
-int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, feab_pcg_result* result, cudaStream_t s) {
+int normalize_lpg(int lpg) { return lpg == 8 || lpg == 16 || lpg == 32 ? lpg : 16; }
+
+int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, feab_pcg_result* result,
+                cudaStream_t s) {
   const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
   static thread_local HostFlag flag;
   if (!flag.ptr) return FEAB_CUDA_ERROR;
-  if (prec == FEAB_PREC_FP32) launch_setup<FEAB_PREC_FP32>(A, gr, s);
-  else if (prec == FEAB_PREC_MIXED) launch_setup<FEAB_PREC_MIXED>(A, gr, s);
-  else launch_setup<FEAB_PREC_FP64>(A, gr, s);
+  if (prec == FEAB_PREC_FP32) launch_setup<FEAB_PREC_FP32>(A, gr, lpg, s);
+  else if (prec == FEAB_PREC_MIXED) launch_setup<FEAB_PREC_MIXED>(A, gr, lpg, s);
+  else launch_setup<FEAB_PREC_FP64>(A, gr, lpg, s);
   FEAB_CHECK_LAUNCH();
 
   cudaStream_t cs = nullptr;
@@ -709,9 +764,9 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, feab_pcg_res
     if (fail(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) break;
     if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
     for (int c = 0; c < chunk; ++c) {
-      if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, cs);
-      else if (prec == FEAB_PREC_MIXED) launch_step<FEAB_PREC_MIXED>(A, gr, cs);
-      else launch_step<FEAB_PREC_FP64>(A, gr, cs);
+      if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, lpg, cs);
+      else if (prec == FEAB_PREC_MIXED) launch_step<FEAB_PREC_MIXED>(A, gr, lpg, cs);
+      else launch_step<FEAB_PREC_FP64>(A, gr, lpg, cs);
     }
     cudaMemcpyAsync((void*)flag.ptr, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
     if (fail(cudaStreamEndCapture(cs, &graph))) break;
@@ -880,11 +935,11 @@ extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* D
   } else {
     FEAB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * M->n, s));
   }
-  return run_pcg(A, prec, chunk, maxiter, result, s);
+  return run_pcg(A, prec, chunk, maxiter, normalize_lpg(prm->lanes_per_group), result, s);
 }
 
-extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Dop, int32_t precision, const void* x,
-                                 void* y, cudaStream_t s) {
+extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Dop, int32_t precision,
+                                 int32_t lanes_per_group, const void* x, void* y, cudaStream_t s) {
   if (!M || !x || !y || M->n <= 0 || !M->row_ptr || !M->col_idx) return FEAB_BAD_ARG;
   if (precision < FEAB_PREC_FP64 || precision > FEAB_PREC_FP32) return FEAB_BAD_ARG;
   if (precision == FEAB_PREC_FP32 ? !M->vals32 : !M->vals64) return FEAB_BAD_ARG;
@@ -893,13 +948,24 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Do
   PcgArgs A{};
   fill_matrix(M, &A);
   const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
+  const int lpg = normalize_lpg(lanes_per_group);
+  const double* xd = static_cast<const double*>(x);
+  double* yd = static_cast<double*>(y);
+  const float* xf = static_cast<const float*>(x);
+  float* yf = static_cast<float*>(y);
   if (precision == FEAB_PREC_FP64) {
-    k_spmv<double><<<gr.a, kThreads, 0, s>>>(A, static_cast<const double*>(x), static_cast<double*>(y));
+    if (lpg == 8) k_spmv<double, 8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else if (lpg == 16) k_spmv<double, 16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else k_spmv<double, 32><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
   } else if (precision == FEAB_PREC_FP32) {
-    k_spmv<float><<<gr.a, kThreads, 0, s>>>(A, static_cast<const float*>(x), static_cast<float*>(y));
+    if (lpg == 8) k_spmv<float, 8><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
+    else if (lpg == 16) k_spmv<float, 16><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
+    else k_spmv<float, 32><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
   } else {
     fill_diff(Dop, &A);
-    k_spmv_diff<<<gr.a, kThreads, 0, s>>>(A, static_cast<const double*>(x), static_cast<double*>(y));
+    if (lpg == 8) k_spmv_diff<8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else if (lpg == 16) k_spmv_diff<16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else k_spmv_diff<32><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
   }
   count_launches(1);
   FEAB_CHECK_LAUNCH();

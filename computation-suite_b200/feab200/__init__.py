@@ -13,8 +13,9 @@ from .material import D_solid3d, Material
 from .mesh import Mesh, box_mesh
 from .solver import FESystem
 from .iterative_solvers import jacobi_preconditioner, preconditioned_cg
-from . import cantilever, facet_loads, topopt  # noqa: F401
+from .batched import ProblemBatch, solve_static_batched
+from . import batched, cantilever, facet_loads, topopt  # noqa: F401
 
 __all__ = ["FESystem", "Mesh", "box_mesh", "Material", "D_solid3d", "Hex8Solid3D", "FEField", "DeviceMesh",
            "ReducedOperator", "SolveInfo", "pcg_solve", "preconditioned_cg", "jacobi_preconditioner",
-           "cantilever", "facet_loads", "topopt"]
+           "ProblemBatch", "solve_static_batched", "batched", "cantilever", "facet_loads", "topopt"]

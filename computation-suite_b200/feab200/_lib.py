@@ -44,9 +44,16 @@ class DiffOperator(C.Structure):
                 ("S", C.c_void_p)]
 
 
+class Batch(C.Structure):
+    _fields_ = [("n_problems", C.c_int32), ("k", C.c_int32), ("n_items", C.c_int32), ("reserved", C.c_int32),
+                ("item_problem", C.c_void_p), ("item_group0", C.c_void_p), ("item_group1", C.c_void_p),
+                ("problem_items", C.c_void_p), ("problem_cols", C.c_void_p)]
+
+
 class PcgParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxiter", C.c_int32), ("precision", C.c_int32),
-                ("reliable_delta", C.c_double), ("chunk", C.c_int32), ("use_dinv", C.c_int32)]
+                ("reliable_delta", C.c_double), ("chunk", C.c_int32), ("use_dinv", C.c_int32),
+                ("lanes_per_group", C.c_int32), ("reserved", C.c_int32)]
 
 
 class PcgResult(C.Structure):
@@ -78,7 +85,14 @@ SIGNATURES = {
     "feab_diff_operator_build": (_I32, [C.POINTER(CSR), _P, _P, _SZ, C.POINTER(DiffOperator), _P]),
     "feab_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _P, _P, _P, _P, _P, C.POINTER(PcgParams), _P,
                               _SZ, C.POINTER(PcgResult), _P]),
-    "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _I32, _P, _P, _P]),
+    "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _I32, _I32, _P, _P, _P]),
+    "feab_block_pcg_workspace_bytes": (_SZ, [_I32, _I32, _I32, _I32]),
+    "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(Batch), _P, _P, _P,
+                                    C.POINTER(PcgParams), _P, _SZ, C.POINTER(_I32), C.POINTER(_D), C.POINTER(_I32),
+                                    _P]),
+    "feab_gram_workspace_bytes": (_SZ, [_I64, _I32]),
+    "feab_gram_bf16x3": (_I32, [_P, _I64, _I32, _P, _P, _SZ, _P, _P]),
+    "feab_symeig_jacobi": (_I32, [_P, _I32, _P, _P, _I32, _P, _P]),
     "feab_hex8_simp_vjp": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _D, _P, _P, _P, _P, _P]),
 }
 

@@ -1,0 +1,196 @@
+"""Batched multi-RHS solves on the GPU.
+
+``solve_static_batched(fesystem, F_batch)`` keeps the reference's signature and meaning
+(fea_engine/src/fea_engine/batched_solve.py:105-164): every column of F_batch is solved against
+the system's K with its boundary conditions (non-homogeneous Dirichlet values included); the
+one factorisation the reference reuses across columns is replaced by a block-PCG whose SpMM
+reads K once per step for the whole panel of columns.
+
+``ProblemBatch`` solves many independent problems (different meshes, moduli and load panels)
+in one launch sequence: the meshes are concatenated into one disconnected mesh, so node
+topology, CSR pattern, element matrices and assembly each run once over the whole batch, and
+K is block diagonal by construction.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .device import DeviceMesh, ReducedOperator, cuda_device
+
+PANELS = (1, 2, 4, 8, 16, 32, 64)
+
+
+def panel_width(k):
+    for w in PANELS:
+        if k <= w:
+            return w
+    raise ValueError(f"at most {PANELS[-1]} right-hand sides per problem in one panel, got {k}")
+
+
+@dataclass
+class BatchResult:
+    status: np.ndarray        # (P,) FEAB_* per problem
+    iters: np.ndarray         # (P, K) CG iterations per column
+    relres: np.ndarray        # (P, K) final FP64 relative residual per column
+
+
+def _work_items(group_ptr_host, row_bounds, max_groups=64):
+    """Cut each problem's node row groups into items of <= max_groups groups."""
+    gp = np.asarray(group_ptr_host, dtype=np.int64)
+    g_bounds = np.searchsorted(gp, row_bounds, side="left")
+    item_problem, g0s, g1s, prob_items = [], [], [], [0]
+    for p in range(len(row_bounds) - 1):
+        a, b = int(g_bounds[p]), int(g_bounds[p + 1])
+        if b <= a:
+            raise ValueError(f"problem {p} has no free DOF")
+        for s in range(a, b, max_groups):
+            item_problem.append(p)
+            g0s.append(s)
+            g1s.append(min(b, s + max_groups))
+        prob_items.append(len(item_problem))
+    return (np.array(item_problem, np.int32), np.array(g0s, np.int32), np.array(g1s, np.int32),
+            np.array(prob_items, np.int32))
+
+
+def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=None, precision="fp64",
+              reliable_delta=0.1, chunk=16, max_groups=64):
+    """Solve the panel B_panel (n x K, row-major, device) for the problems whose free rows are
+    [row_bounds[p], row_bounds[p+1]).  Returns (X_panel, BatchResult)."""
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("block PCG precision must be 'fp64' or 'mixed'")
+    dev = op.vals64.device
+    n, K = B_panel.shape
+    if n != op.n or K not in PANELS:
+        raise ValueError(f"panel must be ({op.n}, k) with k in {PANELS}")
+    gp = op.pattern.group_ptr.cpu().numpy()
+    item_problem, g0, g1, prob_items = _work_items(gp, np.asarray(row_bounds), max_groups)
+    P = len(row_bounds) - 1
+    t = lambda a: torch.as_tensor(a).to(dev)  # noqa: E731
+    ip, ig0, ig1, pit, pcols = t(item_problem), t(g0), t(g1), t(prob_items), t(np.asarray(cols, np.int32))
+    batch = L.Batch(P, K, len(item_problem), 0, ip.data_ptr(), ig0.data_ptr(), ig1.data_ptr(), pit.data_ptr(),
+                    pcols.data_ptr())
+    wbytes = int(L.lib.feab_block_pcg_workspace_bytes(n, K, P, len(item_problem)))
+    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    X = torch.empty((n, K), dtype=torch.float64, device=dev)
+    B_panel = B_panel.to(dev, torch.float64).contiguous()
+    prec = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
+    diff = C.byref(op.diff_operator()) if precision == "mixed" else None
+    params = L.PcgParams(float(tol), int(maxiter or 0), prec, float(reliable_delta), int(chunk), 1, 0, 0)
+    iters = np.zeros(P * K, np.int32)
+    relres = np.zeros(P * K, np.float64)
+    status = np.zeros(P, np.int32)
+    csr = op.csr_struct()
+    rc = L.lib.feab_block_pcg_solve(C.byref(csr), diff, C.byref(batch), L.dptr(op.dinv64), L.dptr(B_panel),
+                                    L.dptr(X), C.byref(params), L.dptr(ws), wbytes,
+                                    iters.ctypes.data_as(C.POINTER(C.c_int32)),
+                                    relres.ctypes.data_as(C.POINTER(C.c_double)),
+                                    status.ctypes.data_as(C.POINTER(C.c_int32)), L.stream_ptr(dev))
+    if rc in (L.FEAB_BAD_ARG, L.FEAB_CUDA_ERROR):
+        L.raise_for(rc, "block PCG")
+    return X, BatchResult(status, iters.reshape(P, K), relres.reshape(P, K))
+
+
+class ProblemBatch:
+    """Independent hex8 problems solved together.  Each problem is (nodes, elements, D, fixed
+    DOFs, F (n_dof,) or (n_dof, k)); D of every problem must be a positive multiple of the
+    first problem's D (same Poisson ratio, any modulus), which becomes a per-element scale."""
+
+    def __init__(self, problems, device=None):
+        self.device = cuda_device(device)
+        if not problems:
+            raise ValueError("empty problem batch")
+        D_ref = np.asarray(problems[0][2], dtype=float)
+        nodes, elems, scale, fixed, self.sizes = [], [], [], [], []
+        off = 0
+        for (X, el, D, fx, F) in problems:
+            X = np.asarray(X, float)
+            el = np.asarray(el)
+            s = float(np.asarray(D)[0, 0] / D_ref[0, 0])
+            if not (s > 0 and np.allclose(np.asarray(D), s * D_ref, rtol=1e-12, atol=0)):
+                raise ValueError("every problem's D must be a positive multiple of the first problem's D")
+            nodes.append(X)
+            elems.append(el + off)
+            scale.append(np.full(len(el), s))
+            fixed.append(np.asarray(fx, np.int64) + 3 * off)
+            self.sizes.append(len(X))
+            off += len(X)
+        self.node_offsets = np.concatenate([[0], np.cumsum(self.sizes)])
+        self.D_ref = D_ref
+        self.dm = DeviceMesh(np.concatenate(nodes), np.concatenate(elems), device=self.device)
+        self.scale = np.concatenate(scale)
+        self.fixed = np.concatenate(fixed)
+        self.loads = [np.asarray(pr[4], float).reshape(3 * len(pr[0]), -1) for pr in problems]
+        mask = np.ones(3 * off, dtype=bool)
+        mask[self.fixed] = False
+        self.free = np.flatnonzero(mask)
+        self.row_bounds = np.searchsorted(self.free, 3 * self.node_offsets)
+        self.cols = [F.shape[1] for F in self.loads]
+        self.K = panel_width(max(self.cols))
+        self.op = None
+
+    def assemble(self):
+        pat = self.dm.pattern(self.fixed)
+        ke = self.dm.element_stiffness(self.D_ref, scale=self.scale)
+        self.op = self.dm.assemble(ke, pat, want32=False)
+        return self.op
+
+    def rhs_panel(self):
+        n = len(self.free)
+        B = np.zeros((n, self.K))
+        for p, F in enumerate(self.loads):
+            a, b = self.row_bounds[p], self.row_bounds[p + 1]
+            rows = self.free[a:b] - 3 * self.node_offsets[p]
+            B[a:b, : F.shape[1]] = F[rows]
+        return torch.as_tensor(B).to(self.device)
+
+    def solve(self, tol=1e-8, maxiter=None, precision="fp64", reliable_delta=0.1, chunk=16):
+        """Returns ([U_p (n_dof_p, k_p) numpy], BatchResult)."""
+        if self.op is None:
+            self.assemble()
+        X, res = block_pcg(self.op, self.row_bounds, self.rhs_panel(), self.cols, tol=tol, maxiter=maxiter,
+                           precision=precision, reliable_delta=reliable_delta, chunk=chunk)
+        Xh = X.cpu().numpy()
+        out = []
+        for p, F in enumerate(self.loads):
+            a, b = self.row_bounds[p], self.row_bounds[p + 1]
+            U = np.zeros((3 * self.sizes[p], F.shape[1]))
+            U[self.free[a:b] - 3 * self.node_offsets[p]] = Xh[a:b, : F.shape[1]]
+            out.append(U)
+        return out, res
+
+
+def solve_static_batched(fesystem, F_batch, backend=None, tol=1e-10, precision="fp64", maxiter=None):
+    """U_batch (n_dof, n_batch) for every load column, with fesystem's K and boundary
+    conditions (batched_solve.py:105-164).  The direct factorisation is replaced by the GPU
+    block-PCG to relative residual `tol` per column; columns are processed in panels of <= 64."""
+    F_batch = np.asarray(F_batch, dtype=float)
+    if F_batch.ndim != 2 or F_batch.shape[0] != fesystem.n_dof:
+        raise ValueError(f"F_batch must have shape ({fesystem.n_dof}, n_batch)")
+    op = fesystem.reduced_operator(want32=False)
+    free = fesystem.free_dofs
+    fixed = fesystem.fixed_dofs_array
+    u_fixed = fesystem._fixed_dof_values_array(fixed)
+    corr = fesystem._reduced_rhs(np.zeros(fesystem.n_dof)).cpu().numpy()   # = -K[free, fixed] u_fixed
+    U = np.zeros((fesystem.n_dof, F_batch.shape[1]))
+    U[fixed, :] = u_fixed[:, None]
+    for c0 in range(0, F_batch.shape[1], 64):
+        Fc = F_batch[:, c0:c0 + 64]
+        k = Fc.shape[1]
+        K = panel_width(k)
+        B = np.zeros((len(free), K))
+        B[:, :k] = Fc[free] + corr[:, None]
+        X, res = block_pcg(op, [0, len(free)], torch.as_tensor(B), [k], tol=tol, maxiter=maxiter,
+                           precision=precision)
+        st = int(res.status[0])
+        if st == L.FEAB_NOT_SPD:
+            raise np.linalg.LinAlgError("solve_static_batched: K is not SPD")
+        if st == L.FEAB_NOT_CONVERGED:
+            raise RuntimeError("solve_static_batched: block PCG did not converge")
+        L.raise_for(st, "solve_static_batched")
+        U[free, c0:c0 + k] = X.cpu().numpy()[:, :k]
+    return U

@@ -299,8 +299,39 @@ class SolveInfo:
 PRECISIONS = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED, "fp32": L.PREC_FP32}
 
 
+LANES_PER_GROUP = (8, 16, 32)
+_tuned = {}
+
+
+def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", reps=3):
+    """SpMV launch shape picked by timing: lanes per node row group in (8, 16, 32), i.e. how
+    many groups each warp keeps in flight.  Measured once per (n, nnz, precision) with CUDA
+    events around the PCG's own SpMV kernel; the result is cached for the process."""
+    key = (op.n, op.nnz, op.pattern.n_groups, precision, op.vals64.device.index)
+    hit = _tuned.get(key)
+    if hit is not None:
+        return hit
+    dt = torch.float32 if precision == "fp32" else torch.float64
+    x = torch.ones(op.n, dtype=dt, device=op.vals64.device)
+    y = torch.empty_like(x)
+    best, best_t = 16, float("inf")
+    for lpg in LANES_PER_GROUP:
+        spmv(op, x, precision, out=y, lanes_per_group=lpg)          # warm
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            spmv(op, x, precision, out=y, lanes_per_group=lpg)
+        b.record()
+        b.synchronize()
+        t = a.elapsed_time(b)
+        if t < best_t:
+            best, best_t = lpg, t
+    _tuned[key] = best
+    return best
+
+
 def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision="fp64", use_dinv=True,
-              reliable_delta=0.1, chunk=16, out=None, workspace=None):
+              reliable_delta=0.1, chunk=16, out=None, workspace=None, lanes_per_group=None):
     """Jacobi-PCG on the device.  Returns (x, SolveInfo); the caller decides how to treat a
     non-OK status (see ``raise_for``)."""
     if precision not in PRECISIONS:
@@ -323,7 +354,10 @@ def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision
         raise ValueError("fp32 precision needs the FP32 copy of K (assemble with want32=True)")
     diff = C.byref(op.diff_operator()) if precision == "mixed" else None
     csr = op.csr_struct()
-    params = L.PcgParams(float(tol), int(maxiter or 0), prec, float(reliable_delta), int(chunk), 1 if use_dinv else 0)
+    if lanes_per_group is None:
+        lanes_per_group = tuned_lanes_per_group(op, precision)
+    params = L.PcgParams(float(tol), int(maxiter or 0), prec, float(reliable_delta), int(chunk), 1 if use_dinv else 0,
+                         int(lanes_per_group), 0)
     res = L.PcgResult()
     rc = L.lib.feab_pcg_solve(C.byref(csr), diff, L.dptr(op.dinv64), L.dptr(op.dinv32), L.dptr(b), L.dptr(x0), L.dptr(x),
                               C.byref(params), L.dptr(workspace), wbytes, C.byref(res), L.stream_ptr(dev))
@@ -333,7 +367,7 @@ def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision
                         float(res.bnorm), precision, int(res.graph_launches))
 
 
-def spmv(op: ReducedOperator, x, precision="fp64", out=None):
+def spmv(op: ReducedOperator, x, precision="fp64", out=None, lanes_per_group=None):
     """y = K_ff x with the PCG's SpMV kernel (FP64 or FP32 values)."""
     prec = PRECISIONS[precision]
     dt = torch.float32 if precision == "fp32" else torch.float64
@@ -341,6 +375,7 @@ def spmv(op: ReducedOperator, x, precision="fp64", out=None):
     y = out if out is not None else torch.empty(op.n, dtype=dt, device=op.vals64.device)
     csr = op.csr_struct()
     diff = C.byref(op.diff_operator()) if precision == "mixed" else None
-    rc = L.lib.feab_csr_spmv(C.byref(csr), diff, prec, L.dptr(x), L.dptr(y), L.stream_ptr(op.vals64.device))
+    lpg = lanes_per_group if lanes_per_group is not None else tuned_lanes_per_group(op, precision)
+    rc = L.lib.feab_csr_spmv(C.byref(csr), diff, prec, int(lpg), L.dptr(x), L.dptr(y), L.stream_ptr(op.vals64.device))
     L.raise_for(rc, "csr spmv")
     return y

@@ -1,0 +1,107 @@
+"""POD basis of a snapshot panel on the GPU (rom_engine/src/rom_engine/pod.py:100-176).
+
+``PodBasis.fit`` keeps the reference's signature and rank rule (n_modes / energy_threshold,
+_select_rank pod.py:163-176).  The FP64 economy SVD of the reference (pod.py:140-147) is
+replaced by the method of snapshots: the 64 x 64 Gram matrix X^T X on the tensor cores
+(split-bf16 x3 products, FP32 accumulate, FP64 across chunks; feab_gram_bf16x3), its FP64
+eigenvalues by a one-CTA Jacobi solver (feab_symeig_jacobi), singular values sqrt(lambda),
+and modes U = X V / sigma.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from .device import cuda_device
+
+MAX_SNAPSHOTS = 64
+
+
+def gram_bf16x3(X):
+    """G = X^T X (FP64, 64 x 64) of a device panel X (n x 64, FP32, row major)."""
+    X = X.contiguous()
+    if X.dtype != torch.float32 or X.ndim != 2 or X.shape[1] != MAX_SNAPSHOTS:
+        raise ValueError("gram_bf16x3 needs an (n, 64) float32 device panel")
+    dev = X.device
+    n = X.shape[0]
+    wbytes = int(L.lib.feab_gram_workspace_bytes(n, MAX_SNAPSHOTS))
+    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    G = torch.empty((MAX_SNAPSHOTS, MAX_SNAPSHOTS), dtype=torch.float64, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    rc = L.lib.feab_gram_bf16x3(L.dptr(X), n, MAX_SNAPSHOTS, L.dptr(G), L.dptr(ws), wbytes, L.dptr(err),
+                                L.stream_ptr(dev))
+    L.raise_for(rc, "gram_bf16x3")
+    if int(err.item()):
+        raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
+    return G
+
+
+def symeig(G, vectors=True, max_sweeps=40):
+    """Eigenvalues (descending) and eigenvectors of a symmetric FP64 device matrix (k <= 64)."""
+    k = G.shape[0]
+    A = G.contiguous().clone()
+    w = torch.empty(k, dtype=torch.float64, device=G.device)
+    V = torch.empty((k, k), dtype=torch.float64, device=G.device) if vectors else None
+    sweeps = torch.zeros(1, dtype=torch.int32, device=G.device)
+    rc = L.lib.feab_symeig_jacobi(L.dptr(A), k, L.dptr(w), L.dptr(V), int(max_sweeps), L.dptr(sweeps),
+                                  L.stream_ptr(G.device))
+    L.raise_for(rc, "symeig_jacobi")
+    return w, V
+
+
+def _select_rank(S, n_modes, energy_threshold):
+    candidates = []
+    if n_modes is not None:
+        candidates.append(min(int(n_modes), len(S)))
+    if energy_threshold is not None:
+        energy = S ** 2
+        total = np.sum(energy)
+        if total <= 0:
+            candidates.append(1)
+        else:
+            cum = np.cumsum(energy) / total
+            candidates.append(min(int(np.searchsorted(cum, energy_threshold) + 1), len(S)))
+    return max(1, min(candidates))
+
+
+class PodBasis:
+    def __init__(self):
+        self.V = None
+        self.singular_values = None
+        self.n_modes = None
+        self.mass_weighted = False
+        self.M = None
+
+    def fit(self, snapshots, n_modes=None, energy_threshold=None, M=None, device=None):
+        if n_modes is None and energy_threshold is None:
+            raise ValueError("fit() needs at least one of n_modes, energy_threshold")
+        if M is not None:
+            raise NotImplementedError("PodBasis.fit: mass-weighted POD is not on the GPU path")
+        dev = snapshots.device if torch.is_tensor(snapshots) and snapshots.is_cuda else cuda_device(device)
+        X = torch.as_tensor(snapshots).to(dev)
+        if X.ndim != 2:
+            raise ValueError(f"snapshots must be 2-D (n_dof, n_snapshots), got shape {tuple(X.shape)}")
+        n, k = X.shape
+        if k > MAX_SNAPSHOTS:
+            raise NotImplementedError(f"PodBasis.fit: at most {MAX_SNAPSHOTS} snapshots per panel on the GPU path")
+        X32 = torch.zeros((n, MAX_SNAPSHOTS), dtype=torch.float32, device=dev)
+        X32[:, :k] = X.to(torch.float32)
+        G = gram_bf16x3(X32)
+        w, V = symeig(G)
+        S = torch.sqrt(torch.clamp(w[: min(k, n)], min=0.0))
+        S_host = S.cpu().numpy()
+        r = _select_rank(S_host, n_modes, energy_threshold)
+        Vk = V[:k, :r]                                       # eigenvectors of the k x k Gram block
+        inv = torch.where(S[:r] > 0, 1.0 / S[:r], torch.zeros_like(S[:r]))
+        self.V = (X.to(torch.float64) @ Vk) * inv[None, :]   # method of snapshots: U = X V / sigma
+        self.singular_values = S_host
+        self.n_modes = r
+        return self
+
+    def energy_captured(self):
+        energy = self.singular_values ** 2
+        total = np.sum(energy)
+        return 1.0 if total <= 0 else float(np.sum(energy[: self.n_modes]) / total)

@@ -86,6 +86,8 @@ typedef struct feab_pcg_params {
   double reliable_delta;     /* mixed: FP64 residual replacement when ||r|| < delta*rmax  */
   int32_t chunk;             /* iterations per CUDA-graph launch (<= 0: default 16)      */
   int32_t use_dinv;          /* 1: Jacobi preconditioner (method="pcg"), 0: plain CG     */
+  int32_t lanes_per_group;   /* SpMV lanes per node row group: 8, 16 or 32 (else 16)     */
+  int32_t reserved;
 } feab_pcg_params;
 
 typedef struct feab_pcg_result {
@@ -198,8 +200,54 @@ int32_t feab_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const 
  * FEAB_PREC_MIXED: x, y double, difference form (diff != NULL).
  * Replaces the CSR SpMV `A @ p` of preconditioned_cg (iterative_solvers.py:448) /
  * `K_t @ x` of torch_sparse_cg_solve (torch_sparse_solver.py:255-256). */
-int32_t feab_csr_spmv(const feab_csr* A, const feab_diff_operator* diff, int32_t precision, const void* x, void* y,
-                      cudaStream_t stream);
+int32_t feab_csr_spmv(const feab_csr* A, const feab_diff_operator* diff, int32_t precision, int32_t lanes_per_group,
+                      const void* x, void* y, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- batched multi-RHS PCG
+ * Many independent problems in one block-diagonal K (e.g. disconnected meshes assembled as
+ * one mesh), each with a panel of right-hand sides.  Vectors are row-major n x k panels
+ * (k in {1,2,4,8,16,32,64}); problem p owns the row groups of its work items.  Each column
+ * runs its own CG recurrence (preconditioned_cg, iterative_solvers.py:434-481) -- the
+ * iterative counterpart of solve_batched / solve_static_batched (batched_solve.py:44-164),
+ * which factorise once for many columns.  precision: FEAB_PREC_FP64 or FEAB_PREC_MIXED
+ * (diff != NULL).  Synchronous; per-column iterations / FP64 relative residuals and
+ * per-problem status go to the optional host arrays. */
+typedef struct feab_batch {
+  int32_t n_problems;
+  int32_t k;                       /* panel width                                   */
+  int32_t n_items;
+  int32_t reserved;
+  const int32_t* item_problem;     /* n_items: problem of the work item             */
+  const int32_t* item_group0;      /* n_items: first row group                      */
+  const int32_t* item_group1;      /* n_items: one past the last row group          */
+  const int32_t* problem_items;    /* n_problems+1: items of p are [p, p+1)          */
+  const int32_t* problem_cols;     /* n_problems: active RHS columns (<= k)          */
+} feab_batch;
+
+size_t feab_block_pcg_workspace_bytes(int32_t n, int32_t k, int32_t n_problems, int32_t n_items);
+
+int32_t feab_block_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const feab_batch* batch,
+                             const double* dinv64, const double* B, double* X, const feab_pcg_params* params,
+                             void* workspace, size_t workspace_bytes, int32_t* iters_out, double* relres_out,
+                             int32_t* status_out, cudaStream_t stream);
+
+/* ---------------------------------------------------------------- POD Gram + eigensolve
+ * Replaces the FP64 economy SVD of PodBasis._fit_standard (rom_engine/src/rom_engine/pod.py:
+ * 140-147) for the singular values: G = X^T X with X (n x 64, FP32, row major, 16-byte
+ * aligned) split into bf16 hi + lo on the tensor cores (tcgen05.mma, TMEM accumulator),
+ * G = hi^T hi + hi^T lo + lo^T hi, FP64 across chunks and CTAs (deterministic); then the FP64
+ * eigenvalues of G (squared singular values).  *error_flag (device int, zero it first) is
+ * set if a bounded wait timed out. */
+size_t feab_gram_workspace_bytes(int64_t n, int32_t k);
+
+int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double* G, void* workspace, size_t workspace_bytes,
+                         int32_t* error_flag, cudaStream_t stream);
+
+/* Cyclic Jacobi eigensolver (one CTA, FP64) for a symmetric k x k matrix (k <= 64) in device
+ * memory: eigenvalues descending into evals, eigenvectors (columns) into evecs (may be NULL).
+ * A is overwritten.  *sweeps_out (device int, may be NULL) receives the sweeps used. */
+int32_t feab_symeig_jacobi(double* A, int32_t k, double* evals, double* evecs, int32_t max_sweeps,
+                           int32_t* sweeps_out, cudaStream_t stream);
 
 /* ---------------------------------------------------------------- SIMP adjoint
  * out[e] = -p (1-rho_min) rho_e^(p-1) * lam_e^T K0_e u_e, with K0_e recomputed from the

@@ -1,0 +1,71 @@
+"""Batched multi-RHS block-PCG against independent per-column oracle solves
+(the reference's batched == independent check, fea_engine/tests/test_batched_solve.py:66-115)."""
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+UTOL = 1e-8
+
+
+def _oracle_columns(c, tol=1e-12):
+    X, el = c.mesh.nodes, c.mesh.elements
+    Kff = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(X[el], c.D), el, 3 * len(X)), c.free)
+    dinv = O.jacobi_inverse_diagonal(Kff)
+    F = c.F.reshape(3 * len(X), -1)
+    U = np.zeros_like(F)
+    for j in range(F.shape[1]):
+        U[c.free, j] = O.preconditioned_cg(Kff, F[c.free, j], dinv, tol=tol)[0]
+    return U
+
+
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_problem_batch_matches_independent_solves(precision):
+    from feab200 import cantilever
+    from feab200.batched import ProblemBatch
+    probs = cantilever.batch_cantilevers(n_problems=5, seed=21, nx_range=(3, 9), nyz_range=(2, 4), rhs_range=(2, 7))
+    batch = ProblemBatch([(p.mesh.nodes, p.mesh.elements, p.D, p.fixed, p.F) for p in probs])
+    U, res = batch.solve(tol=1e-10, precision=precision)
+    assert (res.status == 0).all(), res.status
+    for p, Up in zip(probs, U):
+        ref = _oracle_columns(p)
+        for j in range(ref.shape[1]):
+            err = np.linalg.norm(Up[:, j] - ref[:, j]) / np.linalg.norm(ref[:, j])
+            assert err < UTOL, (p.meta["shape"], j, err)
+    # padded columns stay inactive
+    assert (res.iters[:, 8:] == 0).all() if res.iters.shape[1] > 8 else True
+
+
+def test_solve_static_batched_drop_in(golden):
+    import feab200
+    g = golden("cantilever_20x4x4")
+    mesh = feab200.Mesh(nodes=g["nodes"], elements=g["elements"])
+    fs = feab200.FESystem(mesh, feab200.Hex8Solid3D(), sparse=True)
+    fs.assemble_stiffness(g["D"])
+    fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+    rng = np.random.default_rng(0)
+    F = np.zeros((fs.n_dof, 5))
+    F[:, 0] = g["F"]
+    F[:, 1:] = rng.standard_normal((fs.n_dof, 4)) * 1e3
+    U = feab200.solve_static_batched(fs, F, tol=1e-11)
+    for j in range(5):
+        fs.F[:] = F[:, j]
+        Uj = np.asarray(fs.solve_static(method="pcg", tol=1e-12))
+        assert np.linalg.norm(U[:, j] - Uj) / np.linalg.norm(Uj) < UTOL
+    assert np.linalg.norm(U[:, 0] - g["U_lu"]) / np.linalg.norm(g["U_lu"]) < UTOL
+
+
+def test_block_pcg_wide_panel_single_problem():
+    """One mesh, 40 load columns (panel width 64) -- the snapshot-set layout."""
+    from feab200 import cantilever
+    from feab200.batched import ProblemBatch
+    c = cantilever.fourier_snapshot_cantilever(12, 3, 3, n_rhs=40, seed=2)
+    batch = ProblemBatch([(c.mesh.nodes, c.mesh.elements, c.D, c.fixed, c.F)])
+    assert batch.K == 64
+    (U,), res = batch.solve(tol=1e-11)
+    assert (res.status == 0).all()
+    ref = _oracle_columns(c)
+    err = np.linalg.norm(U - ref) / np.linalg.norm(ref)
+    assert err < UTOL

@@ -23,6 +23,7 @@ extern "C" const char* feab_status_string(int32_t code) {
     case FEAB_NOT_CONVERGED: return "did not converge";
     case FEAB_CUDA_ERROR: return "CUDA error";
     case FEAB_CAPACITY: return "node valence beyond the kernels' limit";
+    case FEAB_SCRATCH_LIMIT: return "problem too large for the fixed scratch of feab_pcg_solve_noalloc";
     default: return "unknown status";
   }
 }

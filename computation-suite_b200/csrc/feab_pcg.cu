@@ -28,6 +28,7 @@
 //                    folding the correction into an FP64 solution.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 #include "feab_common.cuh"
 
 namespace feab {
@@ -970,4 +971,100 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Do
   count_launches(1);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;
+}
+
+// ---------------------------------------------------------------- allocation-free FP64 PCG
+// Fixed device scratch for feab_pcg_solve_noalloc: the PCG state, the block partials and the
+// five FP64 work vectors live here instead of in caller-provided memory.  Every GPU that loads
+// this library holds the array until the process exits.
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[128] = {};  // device address of g_noalloc_scratch, per device ordinal
+}  // namespace
+
+extern "C" size_t feab_pcg_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
+
+extern "C" int32_t feab_pcg_noalloc_max_n(void) {
+  // largest n whose FP64 workspace layout fits the fixed scratch (layout grows by 40 B per row)
+  int32_t lo = 0, hi = (int32_t)(kNoAllocScratchBytes / (5 * sizeof(double))) + 1;
+  while (lo < hi) {
+    const int32_t mid = lo + (hi - lo + 1) / 2;
+    if (layout(mid, FEAB_PREC_FP64, nullptr, nullptr) <= kNoAllocScratchBytes) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+extern "C" int32_t feab_pcg_solve_noalloc(const feab_csr* M, const double* dinv64, const double* b, const double* x0,
+                                          double* x, const feab_pcg_params* prm, feab_pcg_result* result,
+                                          cudaStream_t s) {
+  if (!M || !prm || !b || !x || M->n <= 0 || !M->row_ptr || !M->col_idx || !M->vals64) return FEAB_BAD_ARG;
+  if (prm->precision != FEAB_PREC_FP64) return FEAB_BAD_ARG;
+  if (prm->use_dinv && !dinv64) return FEAB_BAD_ARG;
+  if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
+  if (!(prm->tol >= 0.0)) return FEAB_BAD_ARG;
+  if (layout(M->n, FEAB_PREC_FP64, nullptr, nullptr) > kNoAllocScratchBytes) return FEAB_SCRATCH_LIMIT;
+  int dev = 0;
+  FEAB_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 128) return FEAB_BAD_ARG;
+  void* scratch = nullptr;
+  {
+    // first call on this device: look up the array's device address (with the device current)
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FEAB_CUDA_ERROR;
+      g_noalloc_ptr[dev] = p;
+    }
+    scratch = g_noalloc_ptr[dev];
+  }
+  PcgArgs A{};
+  layout(M->n, FEAB_PREC_FP64, static_cast<char*>(scratch), &A);
+  fill_matrix(M, &A);
+  A.dinv64 = dinv64;
+  A.b = b;
+  A.x0 = x0;
+  A.x = x;
+  A.use_dinv = prm->use_dinv ? 1 : 0;
+  const int maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
+  const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
+  const int lpg = normalize_lpg(prm->lanes_per_group);
+  const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
+  // the state (including the ticket counters) is rebuilt by every call
+  k_init_state<<<1, 1, 0, s>>>(A.S_, prm->tol, 0.1, maxiter);
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  if (x0) {
+    if (x0 != x) FEAB_CUDA(cudaMemcpyAsync(x, x0, sizeof(double) * M->n, cudaMemcpyDeviceToDevice, s));
+  } else {
+    FEAB_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * M->n, s));
+  }
+  launch_setup<FEAB_PREC_FP64>(A, gr, lpg, s);
+  FEAB_CHECK_LAUNCH();
+  // plain launches in chunks, done flag read into a stack variable after each chunk
+  const int64_t max_chunks = ((int64_t)maxiter + chunk - 1) / chunk + 1;
+  int32_t done = 0;
+  for (int64_t c = 0; c < max_chunks && !done; ++c) {
+    for (int k = 0; k < chunk; ++k) launch_step<FEAB_PREC_FP64>(A, gr, lpg, s);
+    count_launches(2 * (uint64_t)chunk);
+    FEAB_CHECK_LAUNCH();
+    FEAB_CUDA(cudaMemcpyAsync(&done, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    FEAB_CUDA(cudaStreamSynchronize(s));
+  }
+  PcgState hs;
+  FEAB_CUDA(cudaMemcpyAsync(&hs, A.S_, sizeof(PcgState), cudaMemcpyDeviceToHost, s));
+  FEAB_CUDA(cudaStreamSynchronize(s));
+  int32_t st = hs.done ? hs.status : FEAB_NOT_CONVERGED;
+  if (result) {
+    result->status = st;
+    result->iters = hs.iters;
+    result->reliable_updates = 0;
+    result->graph_launches = 0;
+    result->relres = hs.relres;
+    result->bnorm = hs.bnorm;
+  }
+  return st;
 }

@@ -21,6 +21,7 @@ FEAB_NOT_SPD = 4
 FEAB_NOT_CONVERGED = 5
 FEAB_CUDA_ERROR = 6
 FEAB_CAPACITY = 7
+FEAB_SCRATCH_LIMIT = 8
 
 KE_PACKED = 324
 KE_FULL = 576
@@ -85,6 +86,9 @@ SIGNATURES = {
     "feab_diff_operator_build": (_I32, [C.POINTER(CSR), _P, _P, _SZ, C.POINTER(DiffOperator), _P]),
     "feab_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _P, _P, _P, _P, _P, C.POINTER(PcgParams), _P,
                               _SZ, C.POINTER(PcgResult), _P]),
+    "feab_pcg_noalloc_scratch_bytes": (_SZ, []),
+    "feab_pcg_noalloc_max_n": (_I32, []),
+    "feab_pcg_solve_noalloc": (_I32, [C.POINTER(CSR), _P, _P, _P, _P, C.POINTER(PcgParams), C.POINTER(PcgResult), _P]),
     "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _I32, _I32, _P, _P, _P]),
     "feab_block_pcg_workspace_bytes": (_SZ, [_I32, _I32, _I32, _I32]),
     "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(Batch), _P, _P, _P,

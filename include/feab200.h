@@ -36,6 +36,7 @@ extern "C" {
 #define FEAB_NOT_CONVERGED 5        /* RuntimeError iterative_solvers.py:478-481           */
 #define FEAB_CUDA_ERROR 6           /* RuntimeError (CUDA launch / runtime failure)        */
 #define FEAB_CAPACITY 7             /* ValueError  node valence beyond the kernels' limit  */
+#define FEAB_SCRATCH_LIMIT 8        /* ValueError  n beyond feab_pcg_solve_noalloc's fixed scratch */
 
 #define FEAB_HEX8_KE_PACKED 324     /* doubles per element: the 36 upper 3x3 node blocks   */
 #define FEAB_HEX8_KE_FULL 576       /* doubles per element: full 24x24, row major          */
@@ -194,6 +195,28 @@ int32_t feab_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const 
                        const float* dinv32, const double* b, const double* x0, double* x,
                        const feab_pcg_params* params, void* workspace, size_t workspace_bytes,
                        feab_pcg_result* result, cudaStream_t stream);
+
+/* Allocation-free FP64 PCG.  No counterpart in the reference: it exists for callers that
+ * cannot allocate device memory -- a host that hands all device memory to its own pool and
+ * forbids libraries from calling cudaMalloc (which would fail or fragment that pool), a
+ * thread that must not block on the implicit device synchronisation cudaMalloc/cudaFree can
+ * cause, or an environment that forbids allocation after start-up.  Same algorithm, arguments
+ * and result as feab_pcg_solve with precision FEAB_PREC_FP64, but the workspace is a fixed
+ * 32 MiB array in the library's device memory (feab_pcg_noalloc_scratch_bytes), held by every
+ * GPU that loads the library until the process exits; n above feab_pcg_noalloc_max_n() (about
+ * 838 thousand rows) is rejected with FEAB_SCRATCH_LIMIT before anything is launched.  The
+ * function calls no cudaMalloc/cudaFree/cudaHostAlloc and creates no stream, event or graph:
+ * it launches the step kernels in chunks and reads the done flag into a stack variable.
+ * The first call on a device looks up the array's device address (cudaGetSymbolAddress with
+ * that device current); make that first call before any stream capture.  All calls on a device
+ * share the one array and it keeps the previous call's contents (each call re-initialises what
+ * must start at zero), so calls that overlap on the GPU -- on different streams or threads --
+ * race and must be serialised by the caller.  Synchronous. */
+size_t feab_pcg_noalloc_scratch_bytes(void);
+int32_t feab_pcg_noalloc_max_n(void);
+int32_t feab_pcg_solve_noalloc(const feab_csr* A, const double* dinv64, const double* b, const double* x0,
+                               double* x, const feab_pcg_params* params, feab_pcg_result* result,
+                               cudaStream_t stream);
 
 /* y = A x with the PCG's SpMV kernel (same code and launch shape as one PCG step's SpMV).
  * FEAB_PREC_FP64: x, y double, vals64; FEAB_PREC_FP32: x, y float, vals32;

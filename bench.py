@@ -46,6 +46,9 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spmv-reps", type=int, default=20)
+    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram"], default="cantilever",
+                    help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
+                         "adjoint, the uneven batch and the snapshot/POD cases")
     return ap.parse_args()
 
 
@@ -322,11 +325,190 @@ def gpu_index(local):
     return local
 
 
+# ----------------------------------------------------------------------------- other workloads
+def _timed(fn, steps, warmup):
+    import torch
+    for _ in range(warmup):
+        fn()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    for _ in range(steps):
+        out = fn()
+    b.record()
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps, out
+
+
+def workload_simp(args):
+    """SIMP compliance on a 96x32x32 cantilever: assemble K(rho), PCG, dC/drho through the
+    torch.autograd.Function (forward solve + adjoint solve + VJP kernel)."""
+    import torch
+    from feab200 import cantilever, topopt
+    from feab200.device import DeviceMesh
+    c = cantilever.simp_cantilever(96, 32, 32)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dm = DeviceMesh(c.mesh.nodes, c.mesh.elements, device=dev)
+    f = torch.as_tensor(c.F[c.free]).to(dev)
+    rho0 = torch.as_tensor(c.meta["rho"]).to(dev)
+    res = {}
+    grads = {}
+    for prec in ("fp64", "mixed"):
+        prob = topopt.SimpProblem(dm, c.D, c.free, penal=3.0, rho_min=1e-9, tol=args.tol, precision=prec)
+
+        def step():
+            rho = rho0.clone().requires_grad_(True)
+            C = torch.dot(f, prob(rho, f))
+            C.backward()
+            return rho.grad
+
+        ms, g = _timed(step, args.steps, args.warmup)
+        res[prec] = ms
+        grads[prec] = g
+    # checks: closed form on the FP64 u, and central differences at 32 elements
+    prob = topopt.SimpProblem(dm, c.D, c.free, penal=3.0, rho_min=1e-9, tol=1e-13)
+    u = prob.solve_free(rho0, f)
+    dc_closed = dm.simp_vjp(c.D, rho0, 3.0, 1e-9, prob.full(u))
+    rng = np.random.default_rng(0)
+    elems = rng.choice(len(rho0), 32, replace=False)
+    h = 1e-6
+    fd = []
+    for e in elems:
+        rp, rm = rho0.clone(), rho0.clone()
+        rp[e] += h
+        rm[e] -= h
+        fd.append(float((torch.dot(f, prob.solve_free(rp, f)) - torch.dot(f, prob.solve_free(rm, f))) / (2 * h)))
+    fd = np.array(fd)
+    ge = grads["mixed"].cpu().numpy()[elems]
+    return {"metric": "SIMP assemble+PCG+adjoint dC/drho time, 96x32x32 hex8", "value": round(res["mixed"], 3),
+            "unit": "ms", "plain_fp64_ms": round(res["fp64"], 3), "mixed_speedup_vs_fp64": round(res["fp64"] / res["mixed"], 3),
+            "n_elements": len(rho0),
+            "rel_err": {"mixed_grad_vs_closed_form": float(torch.linalg.norm(grads["mixed"] - dc_closed) / torch.linalg.norm(dc_closed)),
+                        "fp64_grad_vs_closed_form": float(torch.linalg.norm(grads["fp64"] - dc_closed) / torch.linalg.norm(dc_closed)),
+                        "mixed_grad_vs_fd_max": float(np.max(np.abs(ge - fd) / np.abs(fd)))}}
+
+
+def workload_batch(args):
+    """256 uneven cantilevers (4-16 load cases each) in one block-PCG."""
+    import torch
+    from feab200 import cantilever
+    from feab200.batched import ProblemBatch
+    probs = cantilever.batch_cantilevers(256)
+    problems = [(p.mesh.nodes, p.mesh.elements, p.D, p.fixed, p.F) for p in probs]
+    res = {}
+    out = {}
+    for prec in ("fp64", "mixed"):
+        def step():
+            b = ProblemBatch(problems)
+            return b.solve(tol=args.tol, precision=prec)
+        ms, (U, r) = _timed(step, max(1, args.steps // 2), 1)
+        res[prec] = ms
+        out[prec] = (U, r)
+    b = ProblemBatch(problems)
+    Ut, rt = b.solve(tol=1e-13, precision="fp64")
+    errs = [np.linalg.norm(u - t) / np.linalg.norm(t) for u, t in zip(out["mixed"][0], Ut)]
+    r = out["mixed"][1]
+    n_dof = sum(3 * len(p.mesh.nodes) for p in probs)
+    n_rhs = sum(p.F.shape[1] for p in probs)
+    return {"metric": "uneven batch block-PCG time (256 cantilevers, 4-16 load cases each)", "value": round(res["mixed"], 3),
+            "unit": "ms", "plain_fp64_ms": round(res["fp64"], 3), "mixed_speedup_vs_fp64": round(res["fp64"] / res["mixed"], 3),
+            "problems": len(probs), "total_dof": n_dof, "total_rhs": n_rhs,
+            "iters": {"max": int(r.iters.max()), "mean_active": float(r.iters[r.iters > 0].mean())},
+            "rel_err_max_vs_fp64_tight": float(max(errs)), "status_ok": bool((r.status == 0).all())}
+
+
+def workload_snapshot(args):
+    """192x48x48 cantilever with 64 Fourier load cases: block-PCG, then POD by the tensor-core
+    Gram (split bf16 x3) and the FP64 Jacobi eigensolve."""
+    import torch
+    from feab200 import cantilever
+    from feab200.batched import ProblemBatch
+    from feab200.pod import gram_bf16x3, symeig
+    c = cantilever.fourier_snapshot_cantilever(192, 48, 48)
+    b = ProblemBatch([(c.mesh.nodes, c.mesh.elements, c.D, c.fixed, c.F)])
+    t0 = time.perf_counter()
+    b.assemble()
+    X, r = None, None
+    from feab200.batched import block_pcg
+    res = {}
+    for prec in ("mixed", "fp64"):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        Xp, rp = block_pcg(b.op, b.row_bounds, b.rhs_panel(), b.cols, tol=args.tol, precision=prec)
+        e1.record()
+        torch.cuda.synchronize()
+        res[prec] = (e0.elapsed_time(e1), Xp, rp)
+    X = res["mixed"][1]
+    X32 = X.to(torch.float32).contiguous()
+    gram_ms, G = _timed(lambda: gram_bf16x3(X32), 5, 2)
+    eig_ms, (w, V) = _timed(lambda: symeig(G), 3, 1)
+    s_gpu = torch.sqrt(torch.clamp(w, min=0)).cpu().numpy()
+    import oracle as O
+    s_ref = O.pod_singular_values(X.cpu().numpy())
+    rel = np.abs(s_gpu[:10] - s_ref[:10]) / s_ref[:10]
+    n, k = X.shape
+    peak, _ = measured_peak()
+    gram_bytes = n * k * 4 + k * k * 8
+    return {"metric": "snapshot block-PCG (64 RHS) + tensor-core Gram POD time, 192x48x48 hex8",
+            "value": round(res["mixed"][0] + gram_ms + eig_ms, 2), "unit": "ms",
+            "block_pcg_ms": {"mixed": round(res["mixed"][0], 2), "fp64": round(res["fp64"][0], 2)},
+            "gram_ms": round(gram_ms, 4), "eig_ms": round(eig_ms, 3),
+            "gram_roofline": {"bound": "hbm", "achieved": round(gram_bytes / (gram_ms * 1e-3) / 1e9, 1), "peak": peak,
+                              "unit": "GB/s", "frac": round(gram_bytes / (gram_ms * 1e-3) / 1e9 / peak, 3),
+                              "bytes_per_launch": int(gram_bytes)},
+            "n_free": n, "rhs": int(c.F.shape[1]), "iters_max": int(res["mixed"][2].iters.max()),
+            "sigma_rel_err_top10": [float(v) for v in rel],
+            "x_mixed_vs_fp64": float(torch.linalg.norm(res["mixed"][1] - res["fp64"][1]) / torch.linalg.norm(res["fp64"][1]))}
+
+
+def workload_gram(args):
+    """The tensor-core Gram + FP64 eigensolve alone on a seeded random 1,382,976 x 64 FP32 panel
+    (the snapshot set's size), L2 flushed before each timed launch."""
+    import torch
+    from feab200.pod import gram_bf16x3, symeig
+    n, k = 1_382_976, 64
+    g = torch.Generator(device="cuda").manual_seed(5)
+    X = torch.randn((n, k), generator=g, device="cuda", dtype=torch.float32)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    for _ in range(args.warmup):
+        gram_bf16x3(X)
+    times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        G = gram_bf16x3(X)
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    ms = statistics.mean(times)
+    ref = X.double().T @ X.double()
+    err = float((G - ref).abs().max() / ref.abs().max())
+    w, _ = symeig(G)
+    peak, kind = measured_peak()
+    nbytes = n * k * 4 + k * k * 8
+    return {"metric": "tensor-core split-bf16 Gram X^T X time, 1382976 x 64 FP32", "value": round(ms, 4), "unit": "ms",
+            "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3), "bytes_per_launch": nbytes,
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})"},
+            "gram_rel_err_vs_fp64": err, "lambda_max": float(w[0])}
+
+
 # ----------------------------------------------------------------------------- main
 def main():
     args = parse()
     import torch
     world, rank, local = dist_setup(args.gpus)
+    if args.workload != "cantilever" and args.impl == "ours":
+        fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
+              "gram": workload_gram}[args.workload]
+        line = fn(args)
+        line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
+                     "data": "synthetic", "workload": args.workload})
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     shape = tuple(args.shape)
     workload = (f"cantilever hex8 {shape[0]}x{shape[1]}x{shape[2]} (2.0x0.4x0.4 m, random tip traction, "
                 f"x=0 clamped): topology+pattern+Ke+CSR assembly + Jacobi-PCG (rel residual {args.tol:g}) "
@@ -358,8 +540,8 @@ def main():
     prob = DeviceProblem(c, dev)
     clocks = ClockSampler(gpu_index(local))
     # plain FP64 first, then mixed (the headline)
-    ms64, x64, dc64, info64, op64, _ = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
     clocks.start()
+    ms64, x64, dc64, info64, op64, _ = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
     ms32, x32, dc32, info32, op, launches = time_steps(prob, "mixed", args.tol, args.steps, args.warmup, world)
     clk = clocks.stop()
     # the FP32-everything variant, one solve, for reference

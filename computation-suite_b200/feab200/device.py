@@ -303,27 +303,26 @@ LANES_PER_GROUP = (8, 16, 32)
 _tuned = {}
 
 
-def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", reps=3):
+def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", iters=24, b=None):
     """SpMV launch shape picked by timing: lanes per node row group in (8, 16, 32), i.e. how
-    many groups each warp keeps in flight.  Measured once per (n, nnz, precision) with CUDA
-    events around the PCG's own SpMV kernel; the result is cached for the process."""
+    many node groups each warp keeps in flight.  Each candidate runs `iters` iterations of the
+    PCG itself (the fused step kernels, not a bare SpMV), timed with CUDA events on the current
+    stream; the fastest is cached for the process per (n, nnz, groups, precision, device)."""
     key = (op.n, op.nnz, op.pattern.n_groups, precision, op.vals64.device.index)
     hit = _tuned.get(key)
     if hit is not None:
         return hit
-    dt = torch.float32 if precision == "fp32" else torch.float64
-    x = torch.ones(op.n, dtype=dt, device=op.vals64.device)
-    y = torch.empty_like(x)
+    dev = op.vals64.device
+    rhs = torch.ones(op.n, dtype=torch.float64, device=dev) if b is None else b
     best, best_t = 16, float("inf")
     for lpg in LANES_PER_GROUP:
-        spmv(op, x, precision, out=y, lanes_per_group=lpg)          # warm
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        pcg_solve(op, rhs, tol=0.0, maxiter=4, precision=precision, lanes_per_group=lpg)   # load the kernels
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        for _ in range(reps):
-            spmv(op, x, precision, out=y, lanes_per_group=lpg)
-        b.record()
-        b.synchronize()
-        t = a.elapsed_time(b)
+        pcg_solve(op, rhs, tol=0.0, maxiter=iters, precision=precision, lanes_per_group=lpg, chunk=8)
+        e.record()
+        e.synchronize()
+        t = a.elapsed_time(e)
         if t < best_t:
             best, best_t = lpg, t
     _tuned[key] = best

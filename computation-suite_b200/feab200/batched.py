@@ -57,6 +57,29 @@ def _work_items(group_ptr_host, row_bounds, max_groups=64):
             np.array(prob_items, np.int32))
 
 
+def shard_problems(costs, world):
+    """Assign independent problems to `world` ranks: longest cost first, each to the least
+    loaded rank (ties to the lowest rank).  Deterministic, so every rank computes the same
+    assignment with no communication.  Returns one ascending index array per rank."""
+    costs = np.asarray(costs, dtype=np.float64)
+    if world < 1:
+        raise ValueError("world must be >= 1")
+    order = sorted(range(len(costs)), key=lambda i: (-costs[i], i))
+    load = np.zeros(world)
+    shards = [[] for _ in range(world)]
+    for i in order:
+        r = int(np.argmin(load))
+        shards[r].append(i)
+        load[r] += costs[i]
+    return [np.array(sorted(s), dtype=np.int64) for s in shards]
+
+
+def problem_cost(n_nodes, n_rhs):
+    """Work of one problem in a block-PCG panel: rows x panel width (the SpMM streams K once per
+    step for the whole panel; iteration counts are similar across the batch)."""
+    return 3.0 * n_nodes * panel_width(n_rhs)
+
+
 def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=None, precision="fp64",
               reliable_delta=0.1, chunk=16, max_groups=64):
     """Solve the panel B_panel (n x K, row-major, device) for the problems whose free rows are

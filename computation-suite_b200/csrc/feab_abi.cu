@@ -11,7 +11,7 @@ void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_rela
 
 extern "C" uint64_t feab_launch_count(void) { return feab::g_launches.load(); }
 
-extern "C" int32_t feab_abi_version(void) { return 1; }
+extern "C" int32_t feab_abi_version(void) { return 2; }
 
 extern "C" const char* feab_status_string(int32_t code) {
   switch (code) {

@@ -50,6 +50,8 @@ struct BArgs {
   const int32_t* tcol;
   const uint8_t* gmask;
   const double* S;
+  const int32_t* goff;
+  const int32_t* voff;
   const double* dinv;
   const int32_t* item_problem;
   const int32_t* item_g0;
@@ -101,7 +103,10 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF p
   constexpr int LW = K >= 32 ? 32 : K;  // lanes per sub-warp
   const int sub = lane / LW, cl = lane % LW;
   const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
-  const int s0 = A.row_ptr[r0], len = A.row_ptr[r0 + 1] - s0;
+  // plain: the CSR rows; difference form: the group's padded off-node columns and values
+  const int s0 = DIFF ? A.voff[g] : A.row_ptr[r0];
+  const int c0 = DIFF ? A.goff[g] : 0;
+  const int len = DIFF ? A.goff[g + 1] - c0 : A.row_ptr[r0 + 1] - s0;
 #pragma unroll
   for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -129,9 +134,9 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF p
         for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * xv;
       }
     } else {
-      const unsigned t = (unsigned)__ldg(A.tcol + s0 + m);
+      const unsigned t = (unsigned)__ldg(A.tcol + c0 + m);
       const int j = (int)(t & 0x3fffffffu), jc = (int)(t >> 30);
-      if (j >= r0 && j < r0 + f) continue;  // own node: K_aa (x_a - x_a) = 0
+      if (j >= r0 && j < r0 + f) continue;  // padding (own node, value 0)
       double w[3];
 #pragma unroll
       for (int k = 0; k < 3; ++k)
@@ -593,6 +598,8 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
     A.vlo = D->vlo;
     A.tcol = D->tcol;
     A.gmask = D->gmask;
+    A.goff = D->goff;
+    A.voff = D->voff;
     A.S = D->S;
   }
   A.dinv = dinv64;

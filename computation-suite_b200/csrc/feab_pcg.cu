@@ -30,6 +30,7 @@
 #include <cmath>
 #include <mutex>
 #include "feab_common.cuh"
+#include "feab_scan.cuh"
 
 namespace feab {
 namespace {
@@ -56,8 +57,10 @@ struct PcgArgs {
   // difference-form operator (mixed)
   const uint32_t* vhi;
   const uint16_t* vlo;
-  const int32_t* tcol;     // column | (DOF component << 30)
+  const int32_t* tcol;     // column | (DOF component << 30), per group padded to quads
   const uint8_t* gmask;    // free-DOF mask of each group's node
+  const int32_t* goff;     // group -> first tagged column
+  const int32_t* voff;     // group -> first value
   const double* S;         // n x 3 row-block sums
   const double* dinv64;
   const float* dinv32;
@@ -112,19 +115,21 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, u
 }
 
 // A row group's rows (r0 .. r0+f-1), the first row's start in col_idx / vals, and its length
-// (all rows of a group have the same length and sit back to back in vals).
+// (all rows of a group have the same length and sit back to back in vals).  For the
+// difference-form operator s0 is the first value (voff), c0 the first tagged column (goff) and
+// len the padded off-node column count (a multiple of 4).
 struct Group {
-  int g, r0, f, s0, len, mask;
+  int g, r0, f, s0, c0, len, mask;
   bool valid;
 };
 
 // Visits every row group.  Each warp owns tiles of 32 consecutive groups; lane l loads the
-// descriptor of the tile's l-th group (group_ptr -> row_ptr, plus the free-DOF mask when
-// `with_mask`), so the two dependent pointer loads are paid once per 32 groups.  The warp is
+// descriptor of the tile's l-th group (group_ptr -> row_ptr, or for the difference form
+// goff / voff and the free-DOF mask), so the dependent pointer loads are paid once per 32 groups.  The warp is
 // split into 32/LPG sub-warps of LPG lanes; sub-warp s takes groups s, s + 32/LPG, ... of the
 // tile, so 32/LPG groups have their loads in flight at once.  Lanes of a sub-warp with no group
 // left get len = 0 (they still join the sub-warp's shuffles) and `valid` false.
-template <int LPG, bool with_mask, typename F>
+template <int LPG, bool DIFF, typename F>
 __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn) {
   constexpr int NSG = 32 / LPG;
   const int G = A.group_ptr ? A.n_groups : A.n;
@@ -133,7 +138,7 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
   const int sg = lane / LPG;
   for (int tile = wg; tile < ntiles; tile += nw) {
     const int g = (tile << 5) + lane;
-    int r0 = 0, f = 0, s0 = 0, len = 0, mask = 0;
+    int r0 = 0, f = 0, s0 = 0, c0 = 0, len = 0, mask = 0;
     if (g < G) {
       if (A.group_ptr) {
         r0 = __ldg(A.group_ptr + g);
@@ -142,9 +147,15 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
         r0 = g;
         f = 1;
       }
-      s0 = __ldg(A.row_ptr + r0);
-      len = __ldg(A.row_ptr + r0 + 1) - s0;
-      if (with_mask) mask = A.gmask[g];
+      if (DIFF) {
+        s0 = __ldg(A.voff + g);
+        c0 = __ldg(A.goff + g);
+        len = __ldg(A.goff + g + 1) - c0;
+        mask = __ldg(A.gmask + g);
+      } else {
+        s0 = __ldg(A.row_ptr + r0);
+        len = __ldg(A.row_ptr + r0 + 1) - s0;
+      }
     }
     const int cnt = min(32, G - (tile << 5));
     for (int i = 0; i < cnt; i += NSG) {
@@ -154,8 +165,9 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
       gr.r0 = __shfl_sync(FEAB_FULL_MASK, r0, src);
       gr.f = __shfl_sync(FEAB_FULL_MASK, f, src);
       gr.s0 = __shfl_sync(FEAB_FULL_MASK, s0, src);
+      gr.c0 = DIFF ? __shfl_sync(FEAB_FULL_MASK, c0, src) : 0;
       gr.len = __shfl_sync(FEAB_FULL_MASK, len, src);
-      gr.mask = with_mask ? __shfl_sync(FEAB_FULL_MASK, mask, src) : 0;
+      gr.mask = DIFF ? __shfl_sync(FEAB_FULL_MASK, mask, src) : 0;
       gr.valid = i + sg < cnt;
       if (!gr.valid) {
         gr.f = 0;
@@ -218,46 +230,45 @@ __device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
   return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
 }
 
+__device__ __forceinline__ double dec48q(uint32_t hi, uint32_t lo2, int half) {
+  return dec48(hi, (uint16_t)(half ? lo2 >> 16 : lo2 & 0xffffu));
+}
+
 // Difference-form SpMV over one group with 48-bit values:
-// acc[k] = sum_{c, col(c) not in own node} v[c] (x(col c) - xs[j(c)]) + sum_j S[r0+k][j] xs[j].
-// Values are loaded for every column (own-node columns are multiplied by zero) so that the
-// value loads do not wait for the column loads.
+// acc[k] = sum_{c off-node} v[k][c] (x(col c) - xs[j(c)]) + sum_j S[r0+k][j] xs[j].
+// The group's off-node columns come in quads; a lane takes whole quads (hl, hl + LPG, ...), so
+// each quad is one 16-byte tagged-column load and, per row, one 16-byte + one 8-byte value
+// load.  Padding columns point at the node's first free DOF with value 0 (d = 0 exactly).
 template <int LPG, typename XF>
 __device__ __forceinline__ void group_spmv_diff(const PcgArgs& A, const Group& G, int hl, XF xf, double (&acc)[3]) {
-  const int r0 = G.r0, f = G.f, len = G.len, mask = G.mask;
-  const int32_t* __restrict__ col = A.tcol + G.s0;
-  const uint32_t* __restrict__ hi = A.vhi + G.s0;
-  const uint16_t* __restrict__ lo = A.vlo + G.s0;
+  const int r0 = G.r0, f = G.f, mask = G.mask;
+  const int nq = G.len >> 2;
+  const uint4* __restrict__ tq = reinterpret_cast<const uint4*>(A.tcol + G.c0);
+  const uint4* __restrict__ hq = reinterpret_cast<const uint4*>(A.vhi + G.s0);
+  const uint2* __restrict__ lq = reinterpret_cast<const uint2*>(A.vlo + G.s0);
   double xs[3];
 #pragma unroll
   for (int j = 0; j < 3; ++j) xs[j] = (G.valid && ((mask >> j) & 1)) ? xf(r0 + __popc(mask & ((1 << j) - 1))) : 0.0;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int c0 = hl; c0 < len; c0 += 3 * LPG) {
-    unsigned t[3];
-    uint32_t h[3][3];
-    uint16_t l[3][3];
+  for (int q = hl; q < nq; q += LPG) {
+    const uint4 t = __ldg(tq + q);
+    uint4 h[3];
+    uint2 l[3];
 #pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const int c = c0 + LPG * u;
-      const bool ok = c < len;
-      t[u] = ok ? (unsigned)__ldg(col + c) : 0u;
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const bool okk = ok && k < f;
-        h[k][u] = okk ? __ldg(hi + k * len + c) : 0u;
-        l[k][u] = okk ? __ldg(lo + k * len + c) : (uint16_t)0;
-      }
+    for (int k = 0; k < 3; ++k) {
+      h[k] = k < f ? __ldg(hq + k * nq + q) : make_uint4(0u, 0u, 0u, 0u);
+      l[k] = k < f ? __ldg(lq + k * nq + q) : make_uint2(0u, 0u);
     }
+    const unsigned tt[4] = {t.x, t.y, t.z, t.w};
+    double d[4];
 #pragma unroll
-    for (int u = 0; u < 3; ++u) {
-      const int c = c0 + LPG * u;
-      const int cj = (int)(t[u] & 0x3fffffffu);
-      const bool own = c >= len || (cj >= r0 && cj < r0 + f);
-      const double d = own ? 0.0 : xf(cj) - xs[t[u] >> 30];
-      a0 += dec48(h[0][u], l[0][u]) * d;
-      a1 += dec48(h[1][u], l[1][u]) * d;
-      a2 += dec48(h[2][u], l[2][u]) * d;
-    }
+    for (int i = 0; i < 4; ++i) d[i] = xf((int)(tt[i] & 0x3fffffffu)) - xs[tt[i] >> 30];
+    a0 += dec48q(h[0].x, l[0].x, 0) * d[0] + dec48q(h[0].y, l[0].x, 1) * d[1] + dec48q(h[0].z, l[0].y, 0) * d[2] +
+          dec48q(h[0].w, l[0].y, 1) * d[3];
+    a1 += dec48q(h[1].x, l[1].x, 0) * d[0] + dec48q(h[1].y, l[1].x, 1) * d[1] + dec48q(h[1].z, l[1].y, 0) * d[2] +
+          dec48q(h[1].w, l[1].y, 1) * d[3];
+    a2 += dec48q(h[2].x, l[2].x, 0) * d[0] + dec48q(h[2].y, l[2].x, 1) * d[1] + dec48q(h[2].z, l[2].y, 0) * d[2] +
+          dec48q(h[2].w, l[2].y, 1) * d[3];
   }
   // S[r0+k][j] row-block sums (own-node part of the difference form)
   const double* __restrict__ Sp = A.S + (int64_t)r0 * 3;
@@ -360,7 +371,7 @@ __global__ void __launch_bounds__(kThreads) k_setup_b(PcgArgs A) {
 
 // Step kernel A.
 template <int PREC, int LPG>
-__global__ void __launch_bounds__(kThreads, 4) k_step_a(PcgArgs A) {
+__global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_step_a(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
@@ -585,7 +596,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv(PcgArgs A, const T* __rest
 }
 
 template <int LPG>
-__global__ void __launch_bounds__(kThreads, 4) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
+__global__ void __launch_bounds__(kThreads, 3) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   const int hl = lane % LPG;
   for_each_group<LPG, true>(A, lane, [&](const Group& gr) {
@@ -595,47 +606,87 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv_diff(PcgArgs A, const doub
   });
 }
 
-// Difference-form operator from the FP64 CSR: tagged columns, 48-bit values, group masks and
-// the row-block sums S[r][j] = sum over the row's columns of DOF component j (fixed order).
+// Difference-form operator, pass 1: per group the padded off-node column count Lp (the f own
+// columns leave the list) and the value count f * Lp, scanned afterwards into goff / voff.
+__global__ void k_diff_counts(int32_t n_groups, const int32_t* __restrict__ group_ptr,
+                              const int32_t* __restrict__ row_ptr, int32_t* __restrict__ ccount,
+                              int32_t* __restrict__ vcount) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n_groups) return;
+  const int r0 = group_ptr[g], f = group_ptr[g + 1] - r0;
+  const int len = row_ptr[r0 + 1] - row_ptr[r0];
+  const int lp = (len - f + 3) & ~3;
+  ccount[g] = lp;
+  vcount[g] = f * lp;
+}
+
+// Pass 2, one warp per group: tagged columns, 48-bit values (rounded to nearest on the dropped
+// 16 bits), group masks, and the row-block sums S[r][j] = sum over the row's columns of DOF
+// component j, accumulated in a fixed order (lanes in order, chunks in order).  The node's own
+// columns are the f consecutive entries r0 .. r0+f-1 of the sorted column list.
 __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const int32_t* __restrict__ group_ptr,
                                                          const int32_t* __restrict__ row_ptr,
                                                          const int32_t* __restrict__ col_idx,
                                                          const double* __restrict__ vals,
                                                          const int32_t* __restrict__ dof_of,
+                                                         const int32_t* __restrict__ goff,
+                                                         const int32_t* __restrict__ voff,
                                                          int32_t* __restrict__ tcol, uint32_t* __restrict__ vhi,
                                                          uint16_t* __restrict__ vlo, uint8_t* __restrict__ gmask,
-                                                         double* __restrict__ Ssum) {
+                                                         double* __restrict__ Ssum, int32_t* __restrict__ err) {
   const int lane = threadIdx.x & 31;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   if (g >= n_groups) return;
   const int r0 = group_ptr[g], f = group_ptr[g + 1] - r0;
+  const int c0 = goff[g], lp = goff[g + 1] - c0, v0 = voff[g];
+  const int s00 = row_ptr[r0], len = row_ptr[r0 + 1] - s00;
+  // position of the own columns (the entry equal to r0) in the sorted list
+  int own = -1;
+  for (int cb = 0; cb < len && own < 0; cb += 32) {
+    const int c = cb + lane;
+    const unsigned bal = __ballot_sync(FEAB_FULL_MASK, c < len && col_idx[s00 + c] == r0);
+    if (bal) own = cb + __ffs(bal) - 1;
+  }
+  if (own < 0 || own + f > len || lp < len - f || lp > len - f + 3) {
+    if (lane == 0) atomicExch(err, 1);
+    return;
+  }
+  const int j0 = dof_of[r0] % 3;
   if (lane == 0) {
     int m = 0;
     for (int k = 0; k < f; ++k) m |= 1 << (dof_of[r0 + k] % 3);
     gmask[g] = (uint8_t)m;
   }
   for (int k = 0; k < f; ++k) {
-    const int s0 = row_ptr[r0 + k], len = row_ptr[r0 + k + 1] - s0;
+    const int s0 = row_ptr[r0 + k];
     double sj[3] = {0.0, 0.0, 0.0};
-    for (int c0 = 0; c0 < len; c0 += 32) {
-      const int c = c0 + lane;
+    for (int cb = 0; cb < len; cb += 32) {
+      const int c = cb + lane;
       double v = 0.0;
       int j = 0;
       if (c < len) {
         const int col = col_idx[s0 + c];
         j = dof_of[col] % 3;
         v = vals[s0 + c];
-        if (k == 0) tcol[s0 + c] = (int32_t)((uint32_t)col | ((uint32_t)j << 30));
-        const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
-        vhi[s0 + c] = (uint32_t)(bits >> 32);
-        vlo[s0 + c] = (uint16_t)((bits >> 16) & 0xffffull);
+        if (c < own || c >= own + f) {
+          const int p = c < own ? c : c - f;
+          if (k == 0) tcol[c0 + p] = (int32_t)((uint32_t)col | ((uint32_t)j << 30));
+          const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
+          vhi[v0 + k * lp + p] = (uint32_t)(bits >> 32);
+          vlo[v0 + k * lp + p] = (uint16_t)((bits >> 16) & 0xffffull);
+        }
       }
-      // fixed-order per-row sums: lanes in order, chunks in order
       for (int u = 0; u < 32; ++u) {
         const double vu = __shfl_sync(FEAB_FULL_MASK, v, u);
         const int ju = __shfl_sync(FEAB_FULL_MASK, j, u);
-        if (c0 + u < len) sj[ju] += vu;
+        if (cb + u < len) sj[ju] += vu;
       }
+    }
+    // padding: own first free DOF, value 0
+    for (int p = len - f + lane; p < lp; p += 32) {
+      if (k == 0) tcol[c0 + p] = (int32_t)((uint32_t)r0 | ((uint32_t)j0 << 30));
+      vhi[v0 + k * lp + p] = 0u;
+      vlo[v0 + k * lp + p] = 0;
     }
     if (lane < 3) Ssum[(int64_t)(r0 + k) * 3 + lane] = lane == 0 ? sj[0] : (lane == 1 ? sj[1] : sj[2]);
   }
@@ -722,7 +773,8 @@ struct HostFlag {
 
 template <int PREC>
 void launch_setup(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
-  if (lpg == 8) k_setup_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
+  if (lpg == 4) k_setup_a<PREC, 4><<<gr.a, kThreads, 0, s>>>(A);
+  else if (lpg == 8) k_setup_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
   else if (lpg == 16) k_setup_a<PREC, 16><<<gr.a, kThreads, 0, s>>>(A);
   else k_setup_a<PREC, 32><<<gr.a, kThreads, 0, s>>>(A);
   k_setup_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
@@ -731,13 +783,14 @@ void launch_setup(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
 
 template <int PREC>
 void launch_step(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
-  if (lpg == 8) k_step_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
+  if (lpg == 4) k_step_a<PREC, 4><<<gr.a, kThreads, 0, s>>>(A);
+  else if (lpg == 8) k_step_a<PREC, 8><<<gr.a, kThreads, 0, s>>>(A);
   else if (lpg == 16) k_step_a<PREC, 16><<<gr.a, kThreads, 0, s>>>(A);
   else k_step_a<PREC, 32><<<gr.a, kThreads, 0, s>>>(A);
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
 }
 
-int normalize_lpg(int lpg) { return lpg == 8 || lpg == 16 || lpg == 32 ? lpg : 16; }
+int normalize_lpg(int lpg) { return lpg == 4 || lpg == 8 || lpg == 16 || lpg == 32 ? lpg : 16; }
 
 int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, feab_pcg_result* result,
                 cudaStream_t s) {
@@ -841,26 +894,49 @@ void fill_diff(const feab_diff_operator* D, PcgArgs* A) {
   A->vlo = D->vlo;
   A->gmask = D->gmask;
   A->S = D->S;
+  A->goff = D->goff;
+  A->voff = D->voff;
 }
 
-void diff_layout(int32_t n, int64_t nnz, int32_t n_groups, char* base, feab_diff_operator* D, size_t* total) {
+// Upper bounds from the sizes: sum_g Lp_g <= sum_g (len_g - f_g + 3) <= nnz + 3 G (f_g >= 1) and
+// sum_g f_g Lp_g <= sum_g (f_g len_g - f_g^2 + 3 f_g) <= nnz + 2 G.
+struct DiffScratch {
+  int64_t* scan;
+  int64_t* total;
+  int32_t* err;
+};
+
+void diff_layout(int32_t n, int64_t nnz, int32_t n_groups, char* base, feab_diff_operator* D, size_t* total,
+                 DiffScratch* X = nullptr) {
   size_t off = 0;
   auto take = [&](size_t bytes) {
     char* p = base ? base + off : nullptr;
     off += a256(bytes);
     return p;
   };
-  char* tc = take(sizeof(int32_t) * (size_t)nnz);
-  char* hi = take(sizeof(uint32_t) * (size_t)nnz);
-  char* lo = take(sizeof(uint16_t) * (size_t)nnz);
+  const size_t ncol = (size_t)nnz + 3 * (size_t)n_groups, nval = (size_t)nnz + 2 * (size_t)n_groups;
+  char* tc = take(sizeof(int32_t) * ncol);
+  char* hi = take(sizeof(uint32_t) * nval);
+  char* lo = take(sizeof(uint16_t) * nval);
   char* gm = take((size_t)n_groups);
   char* ss = take(sizeof(double) * 3 * (size_t)n);
+  char* go = take(sizeof(int32_t) * ((size_t)n_groups + 1));
+  char* vo = take(sizeof(int32_t) * ((size_t)n_groups + 1));
+  char* sc = take(sizeof(int64_t) * ((size_t)scan_blocks((int64_t)n_groups + 1) + 2));
+  char* tt = take(sizeof(int64_t) + sizeof(int32_t));
   if (D) {
     D->tcol = reinterpret_cast<int32_t*>(tc);
     D->vhi = reinterpret_cast<uint32_t*>(hi);
     D->vlo = reinterpret_cast<uint16_t*>(lo);
     D->gmask = reinterpret_cast<uint8_t*>(gm);
     D->S = reinterpret_cast<double*>(ss);
+    D->goff = reinterpret_cast<int32_t*>(go);
+    D->voff = reinterpret_cast<int32_t*>(vo);
+  }
+  if (X) {
+    X->scan = reinterpret_cast<int64_t*>(sc);
+    X->total = reinterpret_cast<int64_t*>(tt);
+    X->err = reinterpret_cast<int32_t*>(tt + sizeof(int64_t));
   }
   if (total) *total = off;
 }
@@ -886,16 +962,27 @@ extern "C" int32_t feab_diff_operator_build(const feab_csr* M, const int32_t* do
                                             size_t storage_bytes, feab_diff_operator* out, cudaStream_t s) {
   if (!M || !dof_of || !storage || !out || !M->group_ptr || M->n_groups <= 0 || !M->vals64 || M->n <= 0)
     return FEAB_BAD_ARG;
-  if (M->n >= (1 << 30)) return FEAB_CAPACITY;
+  if (M->n >= (1 << 30) || M->nnz + 3 * (int64_t)M->n_groups >= (int64_t)INT32_MAX) return FEAB_CAPACITY;
   if (feab_diff_operator_bytes(M->n, M->nnz, M->n_groups) > storage_bytes) return FEAB_BAD_ARG;
-  diff_layout(M->n, M->nnz, M->n_groups, static_cast<char*>(storage), out, nullptr);
-  const int wpb = kThreads / 32;
-  k_build_diff<<<(M->n_groups + wpb - 1) / wpb, kThreads, 0, s>>>(M->n_groups, M->group_ptr, M->row_ptr, M->col_idx,
-                                                                   M->vals64, dof_of, out->tcol, out->vhi, out->vlo,
-                                                                   out->gmask, out->S);
+  DiffScratch X;
+  diff_layout(M->n, M->nnz, M->n_groups, static_cast<char*>(storage), out, nullptr, &X);
+  FEAB_CUDA(cudaMemsetAsync(X.err, 0, sizeof(int32_t), s));
+  const int G = M->n_groups;
+  k_diff_counts<<<(G + kThreads - 1) / kThreads, kThreads, 0, s>>>(G, M->group_ptr, M->row_ptr, out->goff, out->voff);
   count_launches(1);
   FEAB_CHECK_LAUNCH();
-  return FEAB_OK;
+  FEAB_CUDA(scan_exclusive_i32(out->goff, out->goff, G, X.scan, X.total, s));
+  FEAB_CUDA(scan_exclusive_i32(out->voff, out->voff, G, X.scan, X.total, s));
+  const int wpb = kThreads / 32;
+  k_build_diff<<<(G + wpb - 1) / wpb, kThreads, 0, s>>>(G, M->group_ptr, M->row_ptr, M->col_idx, M->vals64, dof_of,
+                                                         out->goff, out->voff, out->tcol, out->vhi, out->vlo,
+                                                         out->gmask, out->S, X.err);
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  int32_t err = 0;
+  FEAB_CUDA(cudaMemcpyAsync(&err, X.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  FEAB_CUDA(cudaStreamSynchronize(s));
+  return err ? FEAB_BAD_ARG : FEAB_OK;
 }
 
 extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* Dop, const double* dinv64,
@@ -955,16 +1042,19 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Do
   const float* xf = static_cast<const float*>(x);
   float* yf = static_cast<float*>(y);
   if (precision == FEAB_PREC_FP64) {
-    if (lpg == 8) k_spmv<double, 8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    if (lpg == 4) k_spmv<double, 4><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else if (lpg == 8) k_spmv<double, 8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else if (lpg == 16) k_spmv<double, 16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else k_spmv<double, 32><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
   } else if (precision == FEAB_PREC_FP32) {
-    if (lpg == 8) k_spmv<float, 8><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
+    if (lpg == 4) k_spmv<float, 4><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
+    else if (lpg == 8) k_spmv<float, 8><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
     else if (lpg == 16) k_spmv<float, 16><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
     else k_spmv<float, 32><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
   } else {
     fill_diff(Dop, &A);
-    if (lpg == 8) k_spmv_diff<8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    if (lpg == 4) k_spmv_diff<4><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
+    else if (lpg == 8) k_spmv_diff<8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else if (lpg == 16) k_spmv_diff<16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else k_spmv_diff<32><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
   }

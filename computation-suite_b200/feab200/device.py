@@ -299,7 +299,7 @@ class SolveInfo:
 PRECISIONS = {"fp64": L.PREC_FP64, "mixed": L.PREC_MIXED, "fp32": L.PREC_FP32}
 
 
-LANES_PER_GROUP = (8, 16, 32)
+LANES_PER_GROUP = (4, 8, 16, 32)
 _tuned = {}
 
 

@@ -71,13 +71,19 @@ typedef struct feab_csr {
 
 /* Difference-form operator built from the FP64 CSR by feab_diff_operator_build (storage is
  * caller memory, feab_diff_operator_bytes).  Applies y_a = sum_{b!=a} K_ab (x_b - x_a) + S_a x_a
- * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64. */
+ * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64.
+ * Layout per node row group g (the f rows of one node): its off-node columns, padded to a
+ * multiple of 4 (Lp_g), start at goff[g] in tcol; its values start at voff[g], row-major
+ * (f rows x Lp_g), so every 4-column quad is one 16-byte (vhi) + 8-byte (vlo) load.  Padding
+ * columns point at the node's own first free DOF with value 0. */
 typedef struct feab_diff_operator {
-  int32_t* tcol;     /* nnz: column | (DOF component << 30)             */
-  uint32_t* vhi;     /* nnz: upper 32 bits of the rounded double       */
-  uint16_t* vlo;     /* nnz: next 16 bits                              */
-  uint8_t* gmask;    /* n_groups: free-DOF mask of the group's node    */
-  double* S;         /* 3 n: row-block sums per DOF component          */
+  int32_t* tcol;     /* sum Lp_g: column | (DOF component << 30)            */
+  uint32_t* vhi;     /* sum f_g Lp_g: upper 32 bits of the rounded double   */
+  uint16_t* vlo;     /* sum f_g Lp_g: next 16 bits                          */
+  uint8_t* gmask;    /* n_groups: free-DOF mask of the group's node         */
+  double* S;         /* 3 n: row-block sums per DOF component               */
+  int32_t* goff;     /* n_groups + 1: first tagged column of each group     */
+  int32_t* voff;     /* n_groups + 1: first value of each group             */
 } feab_diff_operator;
 
 typedef struct feab_pcg_params {
@@ -87,7 +93,7 @@ typedef struct feab_pcg_params {
   double reliable_delta;     /* mixed: FP64 residual replacement when ||r|| < delta*rmax  */
   int32_t chunk;             /* iterations per CUDA-graph launch (<= 0: default 16)      */
   int32_t use_dinv;          /* 1: Jacobi preconditioner (method="pcg"), 0: plain CG     */
-  int32_t lanes_per_group;   /* SpMV lanes per node row group: 8, 16 or 32 (else 16)     */
+  int32_t lanes_per_group;   /* SpMV lanes per node row group: 4, 8, 16 or 32 (else 16)  */
   int32_t reserved;
 } feab_pcg_params;
 
@@ -184,6 +190,7 @@ int32_t feab_hex8_apply(const double* ke_packed, const int32_t* conn, const int3
  * Synchronous: returns when the solve has finished; *result holds the outcome. */
 size_t feab_pcg_workspace_bytes(int32_t n, int32_t precision);
 
+/* Upper bound from the sizes alone (no device work); needs nnz + 3 n_groups < 2^31. */
 size_t feab_diff_operator_bytes(int32_t n, int64_t nnz, int32_t n_groups);
 
 /* dof_of[r] = original DOF of reduced row r (free_dofs, solver.py:1400-1401).  A needs

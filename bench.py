@@ -235,28 +235,33 @@ def spmv_bytes(op, precision):
     if precision == "fp32":
         return nnz * 4 + 4 * lead + ptrs + 2 * n * 4
     own = int((f * f).sum())                                   # own-node block entries are skipped
-    return (nnz - own) * 6 + 4 * lead + ptrs + G + 24 * n + 2 * n * 8
+    return (nnz - own) * 6 + 4 * (lead - n) + ptrs + G + 24 * n + 2 * n * 8
 
 
 def spmv_roofline(op, precision, reps, peak_gbs):
-    """Average duration of the PCG's SpMV kernel with CUDA events on the launching stream;
-    L2 is flushed before each launch by a 256 MB write."""
+    """Average duration of the PCG's SpMV kernel (the sliced SELL-32 product for fp64 and mixed,
+    the CSR one for fp32) with CUDA events on the launching stream; L2 is flushed before each
+    launch by a 256 MB write."""
     import torch
-    from feab200.device import spmv
+    from feab200.device import sell_spmv, spmv, tuned_lanes_per_group
     dev = op.vals64.device
     dt = torch.float32 if precision == "fp32" else torch.float64
     x = torch.randn(op.n, dtype=dt, device=dev)
     y = torch.empty(op.n, dtype=dt, device=dev)
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
-    from feab200.device import tuned_lanes_per_group
-    lpg = tuned_lanes_per_group(op, precision)
-    spmv(op, x, precision, out=y, lanes_per_group=lpg)
+    if precision == "fp32":
+        lpg = tuned_lanes_per_group(op, precision)
+        run = lambda: spmv(op, x, precision, out=y, lanes_per_group=lpg)  # noqa: E731
+    else:
+        lpg = None
+        run = lambda: sell_spmv(op, x, precision, out=y)  # noqa: E731
+    run()
     times = []
     for _ in range(reps):
         flush.fill_(1.0)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        spmv(op, x, precision, out=y, lanes_per_group=lpg)
+        run()
         b.record()
         torch.cuda.synchronize()
         times.append(a.elapsed_time(b) * 1e-3)
@@ -265,10 +270,10 @@ def spmv_roofline(op, precision, reps, peak_gbs):
     p = op.pattern
     bytes_csr = p.nnz * ((4 if precision == "fp32" else 8) + 4) + 4 * (p.n + 1) + 2 * p.n * (4 if precision == "fp32" else 8)
     achieved = nbytes / t / 1e9
-    kern = {"fp64": "k_spmv<double>", "fp32": "k_spmv<float>", "mixed": "k_spmv_diff"}[precision]
+    kern = {"fp64": "k_sell_spmv<FP64>", "fp32": f"k_spmv<float, {lpg}>", "mixed": "k_sell_spmv<MIXED>"}[precision]
     return {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak_gbs, "unit": "GB/s",
             "frac": round(achieved / peak_gbs, 3), "traffic": None,
-            "kernel": f"{kern} (the SpMV of PCG step A, {precision}, {lpg} lanes per node group)",
+            "kernel": f"{kern} (the SpMV of PCG step A, {precision})",
             "bytes_per_launch": int(nbytes),
             "csr_formula_bytes": int(bytes_csr), "launch_us": round(t * 1e6, 2)}
 

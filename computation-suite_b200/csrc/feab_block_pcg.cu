@@ -143,7 +143,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF p
         w[k] = k < f ? dec48(__ldg(A.vhi + s0 + k * len + m), __ldg(A.vlo + s0 + k * len + m)) : 0.0;
 #pragma unroll
       for (int q = 0; q < CPL; ++q) {
-        const double d = pf(j, cl + 32 * q, q) - xs[jc][q];
+        const double d = pf(j, cl + 32 * q, q) - (jc == 0 ? xs[0][q] : (jc == 1 ? xs[1][q] : xs[2][q]));
 #pragma unroll
         for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * d;
       }
@@ -272,7 +272,9 @@ __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
       }
       if (lane < LW) {
         const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
-        for (int k = 0; k < f; ++k) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (k >= f) break;
 #pragma unroll
           for (int q = 0; q < CPL; ++q) {
             const int64_t idx = (int64_t)(r0 + k) * K + lane + 32 * q;

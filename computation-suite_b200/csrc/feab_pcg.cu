@@ -1,19 +1,19 @@
 // Jacobi-preconditioned conjugate gradients on the GPU (d).
 //
-// One CG iteration is one "step" of two kernels:
+// CSR path (FP64 or FP32 values): one CG iteration is one "step" of two kernels:
 //   A  p_new = z + beta p_old (formed on the fly inside the SpMV gathers, written for the
 //      warp's own rows into the other half of a p ping-pong buffer), Ap = K p_new, p_new.Ap
 //   B  x += alpha p, r -= alpha Ap, z = M r, r.r and r.z, convergence test, beta
-// The p update is therefore never a separate pass, and its arithmetic is exactly the
-// reference's p = z + beta p.  Scalars live in a device PcgState; each kernel's last block
-// (ticket counter) reduces the per-block partials in a fixed order, so results are
-// bit-reproducible.  A chunk of steps is captured once in a CUDA graph and replayed; kernels
-// return at once when the state says done, and the host polls the done flag one chunk
+// Sliced path (feab_sell_operator, FP64 or mixed values): three kernels,
+//   P  p = z + beta p in place (when a new direction is pending)
+//   A  Ap = K p through the SELL-32 layout, p.Ap
+//   B  as above
+// so the SpMV gathers one vector instead of two.  Either way the arithmetic of the direction
+// update is exactly the reference's p = z + beta p.  Scalars live in a device PcgState; each
+// kernel's last block (ticket counter) reduces the per-block partials in a fixed order, so
+// results are bit-reproducible.  A chunk of steps is captured once in a CUDA graph and replayed;
+// kernels return at once when the state says done, and the host polls the done flag one chunk
 // behind, so there is no host sync per iteration.
-//
-// SpMV: one warp per row group (the rows of one mesh node share their column list), all
-// columns of a group (<= 96 per pass) issued before any is consumed, so each warp keeps a
-// whole group's index, value and gather loads in flight.
 //
 // Precisions (feab_pcg_params.precision):
 //   FEAB_PREC_FP64   the reference recurrence (iterative_solvers.py:434-481) in FP64.
@@ -31,6 +31,7 @@
 #include <mutex>
 #include "feab_common.cuh"
 #include "feab_scan.cuh"
+#include "feab_sell.cuh"
 
 namespace feab {
 namespace {
@@ -54,14 +55,8 @@ struct PcgArgs {
   const int32_t* group_ptr;
   const double* vals64;
   const float* vals32;
-  // difference-form operator (mixed)
-  const uint32_t* vhi;
-  const uint16_t* vlo;
-  const int32_t* tcol;     // column | (DOF component << 30), per group padded to quads
-  const uint8_t* gmask;    // free-DOF mask of each group's node
-  const int32_t* goff;     // group -> first tagged column
-  const int32_t* voff;     // group -> first value
-  const double* S;         // n x 3 row-block sums
+  SellView sell;           // sliced operator (FP64 or mixed values), when use_sell
+  int use_sell;
   const double* dinv64;
   const float* dinv32;
   const double* b;
@@ -115,21 +110,19 @@ __device__ __forceinline__ bool grid_reduce(double (&v)[NV], double* partials, u
 }
 
 // A row group's rows (r0 .. r0+f-1), the first row's start in col_idx / vals, and its length
-// (all rows of a group have the same length and sit back to back in vals).  For the
-// difference-form operator s0 is the first value (voff), c0 the first tagged column (goff) and
-// len the padded off-node column count (a multiple of 4).
+// (all rows of a group have the same length and sit back to back in vals).
 struct Group {
-  int g, r0, f, s0, c0, len, mask;
+  int g, r0, f, s0, len;
   bool valid;
 };
 
 // Visits every row group.  Each warp owns tiles of 32 consecutive groups; lane l loads the
-// descriptor of the tile's l-th group (group_ptr -> row_ptr, or for the difference form
-// goff / voff and the free-DOF mask), so the dependent pointer loads are paid once per 32 groups.  The warp is
+// descriptor of the tile's l-th group (group_ptr -> row_ptr), so the two dependent pointer
+// loads are paid once per 32 groups.  The warp is
 // split into 32/LPG sub-warps of LPG lanes; sub-warp s takes groups s, s + 32/LPG, ... of the
 // tile, so 32/LPG groups have their loads in flight at once.  Lanes of a sub-warp with no group
 // left get len = 0 (they still join the sub-warp's shuffles) and `valid` false.
-template <int LPG, bool DIFF, typename F>
+template <int LPG, typename F>
 __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn) {
   constexpr int NSG = 32 / LPG;
   const int G = A.group_ptr ? A.n_groups : A.n;
@@ -138,7 +131,7 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
   const int sg = lane / LPG;
   for (int tile = wg; tile < ntiles; tile += nw) {
     const int g = (tile << 5) + lane;
-    int r0 = 0, f = 0, s0 = 0, c0 = 0, len = 0, mask = 0;
+    int r0 = 0, f = 0, s0 = 0, len = 0;
     if (g < G) {
       if (A.group_ptr) {
         r0 = __ldg(A.group_ptr + g);
@@ -147,15 +140,8 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
         r0 = g;
         f = 1;
       }
-      if (DIFF) {
-        s0 = __ldg(A.voff + g);
-        c0 = __ldg(A.goff + g);
-        len = __ldg(A.goff + g + 1) - c0;
-        mask = __ldg(A.gmask + g);
-      } else {
-        s0 = __ldg(A.row_ptr + r0);
-        len = __ldg(A.row_ptr + r0 + 1) - s0;
-      }
+      s0 = __ldg(A.row_ptr + r0);
+      len = __ldg(A.row_ptr + r0 + 1) - s0;
     }
     const int cnt = min(32, G - (tile << 5));
     for (int i = 0; i < cnt; i += NSG) {
@@ -165,9 +151,7 @@ __device__ __forceinline__ void for_each_group(const PcgArgs& A, int lane, F fn)
       gr.r0 = __shfl_sync(FEAB_FULL_MASK, r0, src);
       gr.f = __shfl_sync(FEAB_FULL_MASK, f, src);
       gr.s0 = __shfl_sync(FEAB_FULL_MASK, s0, src);
-      gr.c0 = DIFF ? __shfl_sync(FEAB_FULL_MASK, c0, src) : 0;
       gr.len = __shfl_sync(FEAB_FULL_MASK, len, src);
-      gr.mask = DIFF ? __shfl_sync(FEAB_FULL_MASK, mask, src) : 0;
       gr.valid = i + sg < cnt;
       if (!gr.valid) {
         gr.f = 0;
@@ -226,61 +210,6 @@ __device__ __forceinline__ void group_spmv(const PcgArgs& A, const VT* __restric
   acc[2] = seg_sum<LPG>(a2);
 }
 
-__device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
-  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
-}
-
-__device__ __forceinline__ double dec48q(uint32_t hi, uint32_t lo2, int half) {
-  return dec48(hi, (uint16_t)(half ? lo2 >> 16 : lo2 & 0xffffu));
-}
-
-// Difference-form SpMV over one group with 48-bit values:
-// acc[k] = sum_{c off-node} v[k][c] (x(col c) - xs[j(c)]) + sum_j S[r0+k][j] xs[j].
-// The group's off-node columns come in quads; a lane takes whole quads (hl, hl + LPG, ...), so
-// each quad is one 16-byte tagged-column load and, per row, one 16-byte + one 8-byte value
-// load.  Padding columns point at the node's first free DOF with value 0 (d = 0 exactly).
-template <int LPG, typename XF>
-__device__ __forceinline__ void group_spmv_diff(const PcgArgs& A, const Group& G, int hl, XF xf, double (&acc)[3]) {
-  const int r0 = G.r0, f = G.f, mask = G.mask;
-  const int nq = G.len >> 2;
-  const uint4* __restrict__ tq = reinterpret_cast<const uint4*>(A.tcol + G.c0);
-  const uint4* __restrict__ hq = reinterpret_cast<const uint4*>(A.vhi + G.s0);
-  const uint2* __restrict__ lq = reinterpret_cast<const uint2*>(A.vlo + G.s0);
-  double xs[3];
-#pragma unroll
-  for (int j = 0; j < 3; ++j) xs[j] = (G.valid && ((mask >> j) & 1)) ? xf(r0 + __popc(mask & ((1 << j) - 1))) : 0.0;
-  double a0 = 0.0, a1 = 0.0, a2 = 0.0;
-  for (int q = hl; q < nq; q += LPG) {
-    const uint4 t = __ldg(tq + q);
-    uint4 h[3];
-    uint2 l[3];
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      h[k] = k < f ? __ldg(hq + k * nq + q) : make_uint4(0u, 0u, 0u, 0u);
-      l[k] = k < f ? __ldg(lq + k * nq + q) : make_uint2(0u, 0u);
-    }
-    const unsigned tt[4] = {t.x, t.y, t.z, t.w};
-    double d[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) d[i] = xf((int)(tt[i] & 0x3fffffffu)) - xs[tt[i] >> 30];
-    a0 += dec48q(h[0].x, l[0].x, 0) * d[0] + dec48q(h[0].y, l[0].x, 1) * d[1] + dec48q(h[0].z, l[0].y, 0) * d[2] +
-          dec48q(h[0].w, l[0].y, 1) * d[3];
-    a1 += dec48q(h[1].x, l[1].x, 0) * d[0] + dec48q(h[1].y, l[1].x, 1) * d[1] + dec48q(h[1].z, l[1].y, 0) * d[2] +
-          dec48q(h[1].w, l[1].y, 1) * d[3];
-    a2 += dec48q(h[2].x, l[2].x, 0) * d[0] + dec48q(h[2].y, l[2].x, 1) * d[1] + dec48q(h[2].z, l[2].y, 0) * d[2] +
-          dec48q(h[2].w, l[2].y, 1) * d[3];
-  }
-  // S[r0+k][j] row-block sums (own-node part of the difference form)
-  const double* __restrict__ Sp = A.S + (int64_t)r0 * 3;
-  double sx[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k)
-    sx[k] = k < f ? __ldg(Sp + 3 * k) * xs[0] + __ldg(Sp + 3 * k + 1) * xs[1] + __ldg(Sp + 3 * k + 2) * xs[2] : 0.0;
-  acc[0] = seg_sum<LPG>(a0) + sx[0];
-  acc[1] = seg_sum<LPG>(a1) + sx[1];
-  acc[2] = seg_sum<LPG>(a2) + sx[2];
-}
-
 __device__ __forceinline__ double pick3(const double (&a)[3], int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
 __device__ __forceinline__ float pick3(const float (&a)[3], int k) { return k == 0 ? a[0] : (k == 1 ? a[1] : a[2]); }
 
@@ -310,7 +239,7 @@ __global__ void __launch_bounds__(kThreads) k_setup_a(PcgArgs A) {
   const int hl = lane % LPG;
   double* r = PREC == FEAB_PREC_FP32 ? A.r64 : A.r;
   double part[2] = {0.0, 0.0};
-  for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
+  for_each_group<LPG>(A, lane, [&](const Group& gr) {
     double acc[3] = {0.0, 0.0, 0.0};
     if (A.x0) group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.x0 + j); }, acc);
     if (hl < gr.f) {
@@ -369,9 +298,9 @@ __global__ void __launch_bounds__(kThreads) k_setup_b(PcgArgs A) {
   }
 }
 
-// Step kernel A.
+// Step kernel A, CSR path (FP64 or FP32 values).
 template <int PREC, int LPG>
-__global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_step_a(PcgArgs A) {
+__global__ void __launch_bounds__(kThreads, 4) k_step_a(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
@@ -384,7 +313,7 @@ __global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_s
     // r64 = b - K64 (x64 + x32); x64' = x64 + x32 (other half of the ping-pong)
     const double* xin = S->xsel ? A.x64b : A.x64a;
     double* xout = S->xsel ? A.x64a : A.x64b;
-    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
+    for_each_group<LPG>(A, lane, [&](const Group& gr) {
       double acc[3];
       group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(xin + j) + (double)__ldg(A.x32 + j); },
                          acc);
@@ -396,23 +325,11 @@ __global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_s
         part[0] += ri * ri;
       }
     });
-  } else if (PREC == FEAB_PREC_MIXED && mode == kModeReliable) {
-    // FP64 residual with the exact FP64 values: r = b - K64 x
-    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
-      double acc[3];
-      group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.x + j); }, acc);
-      if (hl < gr.f) {
-        const int i = gr.r0 + hl;
-        const double ri = A.b[i] - pick3(acc, hl);
-        A.r[i] = ri;
-        part[0] += ri * ri;
-      }
-    });
   } else if (PREC == FEAB_PREC_FP32) {
     const float beta = (float)S->beta;
     const float* __restrict__ qo = psel ? A.q1 : A.q0;
     float* __restrict__ qn = psel ? A.q0 : A.q1;
-    for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
+    for_each_group<LPG>(A, lane, [&](const Group& gr) {
       float acc[3];
       if (pend) {
         group_spmv<LPG, float>(A, A.vals32, gr, hl, [&](int j) { return fmaf(beta, __ldg(qo + j), __ldg(A.z32 + j)); },
@@ -433,20 +350,13 @@ __global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_s
     const double beta = S->beta;
     const double* __restrict__ po = psel ? A.p1 : A.p0;
     double* __restrict__ pn = psel ? A.p0 : A.p1;
-    for_each_group<LPG, PREC == FEAB_PREC_MIXED>(A, lane, [&](const Group& gr) {
+    for_each_group<LPG>(A, lane, [&](const Group& gr) {
       double acc[3];
-      if (PREC == FEAB_PREC_MIXED) {
-        if (pend)
-          group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc);
-        else
-          group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(po + j); }, acc);
-      } else {
-        if (pend)
-          group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); },
-                             acc);
-        else
-          group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(po + j); }, acc);
-      }
+      if (pend)
+        group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); },
+                                acc);
+      else
+        group_spmv<LPG, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(po + j); }, acc);
       if (hl < gr.f) {
         const int i = gr.r0 + hl;
         const double pi = pend ? A.z[i] + beta * po[i] : po[i];
@@ -463,6 +373,69 @@ __global__ void __launch_bounds__(kThreads, PREC == FEAB_PREC_MIXED ? 3 : 4) k_s
       S->rr64 = tot[0];
     } else {
       if (pend) S->psel = psel ^ 1;
+      S->p_pending = 0;
+      S->pAp = tot[0];
+      if (!(tot[0] > 0.0)) {  // p^T A p <= 0: A is not SPD (iterative_solvers.py:450-454)
+        S->status = FEAB_NOT_SPD;
+        S->done = 1;
+      } else {
+        S->alpha = S->rz_old / tot[0];
+      }
+    }
+  }
+}
+
+// Sliced path, kernel P: p = z + beta p in place when a new direction is pending.
+__global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
+  const PcgState* S = A.S_;
+  if (S->done || !S->p_pending) return;
+  const double beta = S->beta;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
+    A.p0[i] = A.z[i] + beta * A.p0[i];
+}
+
+// Sliced path, kernel A: Ap = K p and p.Ap through the SELL-32 operator (PREC = its kind); in a
+// mixed reliable step, the FP64 residual r = b - K64 x through the CSR values instead.
+template <int PREC>
+__global__ void __launch_bounds__(kThreads, 4) k_step_a_sell(PcgArgs A) {
+  PcgState* S = A.S_;
+  if (S->done) return;
+  const int mode = S->mode;
+  const int lane = threadIdx.x & 31;
+  double part[1] = {0.0};
+  if (PREC == FEAB_PREC_MIXED && mode == kModeReliable) {
+    for_each_group<8>(A, lane, [&](const Group& gr) {
+      double acc[3];
+      const int hl = lane % 8;
+      group_spmv<8, double>(A, A.vals64, gr, hl, [&](int j) { return __ldg(A.x + j); }, acc);
+      if (hl < gr.f) {
+        const int i = gr.r0 + hl;
+        const double ri = A.b[i] - pick3(acc, hl);
+        A.r[i] = ri;
+        part[0] += ri * ri;
+      }
+    });
+  } else {
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < A.sell.n_slices; sl += nw) {
+      const SellLane L = sell_lane(A.sell, sl, lane);
+      double acc[3], xs[3];
+      sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.p0 + j); }, acc, xs);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k < L.f) {
+          const int i = L.r0 + k;
+          A.Ap[i] = acc[k];
+          part[0] += A.p0[i] * acc[k];
+        }
+      }
+    }
+  }
+  double tot[1];
+  if (grid_reduce<1>(part, A.partials, &S->ticket[0], tot) && threadIdx.x == 0) {
+    if (mode == kModeReliable && PREC != FEAB_PREC_FP64) {
+      S->rr64 = tot[0];
+    } else {
       S->p_pending = 0;
       S->pAp = tot[0];
       if (!(tot[0] > 0.0)) {  // p^T A p <= 0: A is not SPD (iterative_solvers.py:450-454)
@@ -588,20 +561,9 @@ __global__ void __launch_bounds__(kThreads, 4) k_spmv(PcgArgs A, const T* __rest
   const T* vals;
   if constexpr (sizeof(T) == 8) vals = reinterpret_cast<const T*>(A.vals64);
   else vals = reinterpret_cast<const T*>(A.vals32);
-  for_each_group<LPG, false>(A, lane, [&](const Group& gr) {
+  for_each_group<LPG>(A, lane, [&](const Group& gr) {
     T acc[3];
     group_spmv<LPG, T>(A, vals, gr, hl, [&](int j) { return __ldg(x + j); }, acc);
-    if (hl < gr.f) y[gr.r0 + hl] = pick3(acc, hl);
-  });
-}
-
-template <int LPG>
-__global__ void __launch_bounds__(kThreads, 3) k_spmv_diff(PcgArgs A, const double* __restrict__ x, double* __restrict__ y) {
-  const int lane = threadIdx.x & 31;
-  const int hl = lane % LPG;
-  for_each_group<LPG, true>(A, lane, [&](const Group& gr) {
-    double acc[3];
-    group_spmv_diff<LPG>(A, gr, hl, [&](int j) { return __ldg(x + j); }, acc);
     if (hl < gr.f) y[gr.r0 + hl] = pick3(acc, hl);
   });
 }
@@ -790,6 +752,19 @@ void launch_step(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
 }
 
+// Sliced path: P, A (one warp per slice of 32 node groups), B.
+int sell_grid(const PcgArgs& A) {
+  const int wpb = kThreads / 32;
+  return std::max(1, std::min((A.sell.n_slices + wpb - 1) / wpb, max_grid()));
+}
+
+template <int PREC>
+void launch_step_sell(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
+  k_step_p<<<gr.b, kThreads, 0, s>>>(A);
+  k_step_a_sell<PREC><<<sell_grid(A), kThreads, 0, s>>>(A);
+  k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
+}
+
 int normalize_lpg(int lpg) { return lpg == 4 || lpg == 8 || lpg == 16 || lpg == 32 ? lpg : 16; }
 
 int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, feab_pcg_result* result,
@@ -819,7 +794,8 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
     if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
     for (int c = 0; c < chunk; ++c) {
       if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, lpg, cs);
-      else if (prec == FEAB_PREC_MIXED) launch_step<FEAB_PREC_MIXED>(A, gr, lpg, cs);
+      else if (prec == FEAB_PREC_MIXED) launch_step_sell<FEAB_PREC_MIXED>(A, gr, cs);
+      else if (A.use_sell) launch_step_sell<FEAB_PREC_FP64>(A, gr, cs);
       else launch_step<FEAB_PREC_FP64>(A, gr, lpg, cs);
     }
     cudaMemcpyAsync((void*)flag.ptr, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
@@ -833,14 +809,15 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
     if (fail(cudaGraphLaunch(exec, s))) break;
     if (fail(cudaEventRecord(ev[0], s))) break;
     launched = 1;
-    count_launches(2 * (uint64_t)chunk);
+    const uint64_t per_step = A.use_sell ? 3 : 2;
+    count_launches(per_step * (uint64_t)chunk);
     while (true) {
       const bool more = launched < max_launch;
       if (more) {
         if (fail(cudaGraphLaunch(exec, s))) break;
         if (fail(cudaEventRecord(ev[launched & 1], s))) break;
         ++launched;
-        count_launches(2 * (uint64_t)chunk);
+        count_launches(per_step * (uint64_t)chunk);
       }
       if (fail(cudaEventSynchronize(ev[more ? ((launched - 2) & 1) : ((launched - 1) & 1)]))) break;
       if (flag.ptr[0] != 0 || !more) break;
@@ -888,14 +865,15 @@ void fill_matrix(const feab_csr* M, PcgArgs* A) {
   A->vals32 = M->vals32;
 }
 
-void fill_diff(const feab_diff_operator* D, PcgArgs* A) {
-  A->tcol = D->tcol;
-  A->vhi = D->vhi;
-  A->vlo = D->vlo;
-  A->gmask = D->gmask;
-  A->S = D->S;
-  A->goff = D->goff;
-  A->voff = D->voff;
+void fill_sell(const feab_csr* M, const feab_sell_operator* D, PcgArgs* A) {
+  A->sell = sell_view(M, D);
+  A->use_sell = 1;
+}
+
+// A sliced operator fits A and is of the kind the precision needs.
+bool sell_fits(const feab_csr* M, const feab_sell_operator* D, int kind) {
+  return D && M->group_ptr && M->n_groups > 0 && D->kind == kind && D->n_slices == (M->n_groups + 31) / 32 &&
+         D->soff && D->tcol && (kind == FEAB_PREC_FP64 ? D->v64 != nullptr : (D->vhi && D->vlo && D->gmask && D->S));
 }
 
 // Upper bounds from the sizes: sum_g Lp_g <= sum_g (len_g - f_g + 3) <= nnz + 3 G (f_g >= 1) and
@@ -985,7 +963,7 @@ extern "C" int32_t feab_diff_operator_build(const feab_csr* M, const int32_t* do
   return err ? FEAB_BAD_ARG : FEAB_OK;
 }
 
-extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* Dop, const double* dinv64,
+extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_sell_operator* sell, const double* dinv64,
                                   const float* dinv32, const double* b, const double* x0, double* x,
                                   const feab_pcg_params* prm, void* workspace, size_t workspace_bytes,
                                   feab_pcg_result* result, cudaStream_t s) {
@@ -994,14 +972,15 @@ extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* D
   const int prec = prm->precision;
   if (prec < FEAB_PREC_FP64 || prec > FEAB_PREC_FP32) return FEAB_BAD_ARG;
   if (prec == FEAB_PREC_FP32 && !M->vals32) return FEAB_BAD_ARG;
-  if (prec == FEAB_PREC_MIXED && (!Dop || !M->group_ptr)) return FEAB_BAD_ARG;
+  if (prec == FEAB_PREC_MIXED && !sell_fits(M, sell, FEAB_PREC_MIXED)) return FEAB_BAD_ARG;
+  if (prec == FEAB_PREC_FP64 && sell && !sell_fits(M, sell, FEAB_PREC_FP64)) return FEAB_BAD_ARG;
   if (prm->use_dinv && (prec == FEAB_PREC_FP32 ? !dinv32 : !dinv64)) return FEAB_BAD_ARG;
   if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
   if (!(prm->tol >= 0.0)) return FEAB_BAD_ARG;
   PcgArgs A{};
   if (layout(M->n, prec, static_cast<char*>(workspace), &A) > workspace_bytes) return FEAB_BAD_ARG;
   fill_matrix(M, &A);
-  if (Dop) fill_diff(Dop, &A);
+  if (sell && prec != FEAB_PREC_FP32) fill_sell(M, sell, &A);
   A.dinv64 = dinv64;
   A.dinv32 = dinv32;
   A.b = b;
@@ -1026,13 +1005,19 @@ extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_diff_operator* D
   return run_pcg(A, prec, chunk, maxiter, normalize_lpg(prm->lanes_per_group), result, s);
 }
 
-extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Dop, int32_t precision,
+extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_sell_operator* sell, int32_t precision,
                                  int32_t lanes_per_group, const void* x, void* y, cudaStream_t s) {
   if (!M || !x || !y || M->n <= 0 || !M->row_ptr || !M->col_idx) return FEAB_BAD_ARG;
   if (precision < FEAB_PREC_FP64 || precision > FEAB_PREC_FP32) return FEAB_BAD_ARG;
   if (precision == FEAB_PREC_FP32 ? !M->vals32 : !M->vals64) return FEAB_BAD_ARG;
-  if (precision == FEAB_PREC_MIXED && (!Dop || !M->group_ptr)) return FEAB_BAD_ARG;
+  if (precision == FEAB_PREC_MIXED && !sell_fits(M, sell, FEAB_PREC_MIXED)) return FEAB_BAD_ARG;
+  if (precision == FEAB_PREC_FP64 && sell && !sell_fits(M, sell, FEAB_PREC_FP64)) return FEAB_BAD_ARG;
   if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
+  if (sell && precision != FEAB_PREC_FP32) {
+    launch_sell_spmv(sell_view(M, sell), static_cast<const double*>(x), static_cast<double*>(y), s);
+    FEAB_CHECK_LAUNCH();
+    return FEAB_OK;
+  }
   PcgArgs A{};
   fill_matrix(M, &A);
   const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
@@ -1041,7 +1026,7 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Do
   double* yd = static_cast<double*>(y);
   const float* xf = static_cast<const float*>(x);
   float* yf = static_cast<float*>(y);
-  if (precision == FEAB_PREC_FP64) {
+  if (precision != FEAB_PREC_FP32) {
     if (lpg == 4) k_spmv<double, 4><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else if (lpg == 8) k_spmv<double, 8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
     else if (lpg == 16) k_spmv<double, 16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
@@ -1051,12 +1036,6 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_diff_operator* Do
     else if (lpg == 8) k_spmv<float, 8><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
     else if (lpg == 16) k_spmv<float, 16><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
     else k_spmv<float, 32><<<gr.a, kThreads, 0, s>>>(A, xf, yf);
-  } else {
-    fill_diff(Dop, &A);
-    if (lpg == 4) k_spmv_diff<4><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
-    else if (lpg == 8) k_spmv_diff<8><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
-    else if (lpg == 16) k_spmv_diff<16><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
-    else k_spmv_diff<32><<<gr.a, kThreads, 0, s>>>(A, xd, yd);
   }
   count_launches(1);
   FEAB_CHECK_LAUNCH();

@@ -45,6 +45,12 @@ class DiffOperator(C.Structure):
                 ("S", C.c_void_p), ("goff", C.c_void_p), ("voff", C.c_void_p)]
 
 
+class SellOperator(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("n_slices", C.c_int32), ("soff", C.c_void_p), ("tcol", C.c_void_p),
+                ("v64", C.c_void_p), ("vhi", C.c_void_p), ("vlo", C.c_void_p), ("gmask", C.c_void_p),
+                ("S", C.c_void_p)]
+
+
 class Batch(C.Structure):
     _fields_ = [("n_problems", C.c_int32), ("k", C.c_int32), ("n_items", C.c_int32), ("reserved", C.c_int32),
                 ("item_problem", C.c_void_p), ("item_group0", C.c_void_p), ("item_group1", C.c_void_p),
@@ -84,12 +90,15 @@ SIGNATURES = {
     "feab_pcg_workspace_bytes": (_SZ, [_I32, _I32]),
     "feab_diff_operator_bytes": (_SZ, [_I32, _I64, _I32]),
     "feab_diff_operator_build": (_I32, [C.POINTER(CSR), _P, _P, _SZ, C.POINTER(DiffOperator), _P]),
-    "feab_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _P, _P, _P, _P, _P, C.POINTER(PcgParams), _P,
+    "feab_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(SellOperator), _P, _P, _P, _P, _P, C.POINTER(PcgParams), _P,
                               _SZ, C.POINTER(PcgResult), _P]),
     "feab_pcg_noalloc_scratch_bytes": (_SZ, []),
     "feab_pcg_noalloc_max_n": (_I32, []),
     "feab_pcg_solve_noalloc": (_I32, [C.POINTER(CSR), _P, _P, _P, _P, C.POINTER(PcgParams), C.POINTER(PcgResult), _P]),
-    "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _I32, _I32, _P, _P, _P]),
+    "feab_sell_operator_bytes": (_SZ, [_I32, _I32, _I32, _I32]),
+    "feab_sell_operator_build": (_I32, [C.POINTER(CSR), _P, _I32, _I32, _P, _SZ, C.POINTER(SellOperator), _P]),
+    "feab_sell_spmv": (_I32, [C.POINTER(CSR), C.POINTER(SellOperator), _P, _P, _P]),
+    "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(SellOperator), _I32, _I32, _P, _P, _P]),
     "feab_block_pcg_workspace_bytes": (_SZ, [_I32, _I32, _I32, _I32]),
     "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(Batch), _P, _P, _P,
                                     C.POINTER(PcgParams), _P, _SZ, C.POINTER(_I32), C.POINTER(_D), C.POINTER(_I32),

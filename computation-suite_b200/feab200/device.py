@@ -78,6 +78,7 @@ class ReducedOperator:
     dinv64: torch.Tensor
     dinv32: torch.Tensor | None
     _diff: object = None
+    _sell: dict = None
 
     def diff_operator(self):
         """The 48-bit difference-form operator (feab_diff_operator_build), cached."""
@@ -96,6 +97,35 @@ class ReducedOperator:
             L.raise_for(rc, "difference-form operator")
             self._diff = (storage, d)
         return self._diff[1]
+
+    def max_row_len(self):
+        rp = self.pattern.row_ptr
+        return int((rp[1:] - rp[:-1]).max().item()) if self.pattern.n > 0 else 0
+
+    def sell_operator(self, precision="fp64"):
+        """The sliced (SELL-32) node-group operator (feab_sell_operator_build) for "fp64"
+        (plain FP64 values) or "mixed" (48-bit values, difference form), cached."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("the sliced operator holds 'fp64' or 'mixed' values")
+        if self._sell is None:
+            self._sell = {}
+        if precision not in self._sell:
+            p = self.pattern
+            if p.group_ptr is None or p.free_map.numel() == 0:
+                raise ValueError("the sliced operator needs node row groups (an assembled K_ff)")
+            dev = self.vals64.device
+            kind = PRECISIONS[precision]
+            mrl = self.max_row_len()
+            dof_of = torch.nonzero(p.free_map >= 0).flatten().to(torch.int32) if precision == "mixed" else None
+            nbytes = int(L.lib.feab_sell_operator_bytes(p.n, p.n_groups, mrl, kind))
+            storage = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+            d = L.SellOperator()
+            csr = self.csr_struct()
+            rc = L.lib.feab_sell_operator_build(C.byref(csr), L.dptr(dof_of), kind, mrl, L.dptr(storage), nbytes,
+                                                C.byref(d), L.stream_ptr(dev))
+            L.raise_for(rc, "sliced operator")
+            self._sell[precision] = (storage, d, dof_of)
+        return self._sell[precision][1]
 
     @property
     def n(self):
@@ -304,10 +334,11 @@ _tuned = {}
 
 
 def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", iters=24, b=None):
-    """SpMV launch shape picked by timing: lanes per node row group in (8, 16, 32), i.e. how
-    many node groups each warp keeps in flight.  Each candidate runs `iters` iterations of the
-    PCG itself (the fused step kernels, not a bare SpMV), timed with CUDA events on the current
-    stream; the fastest is cached for the process per (n, nnz, groups, precision, device)."""
+    """CSR SpMV launch shape picked by timing: lanes per node row group in (4, 8, 16, 32), i.e.
+    how many node groups each warp keeps in flight.  Each candidate runs `iters` iterations of
+    the CSR-layout PCG itself (the fused step kernels, not a bare SpMV), timed with CUDA events
+    on the current stream; the fastest is cached for the process per (n, nnz, groups,
+    precision, device)."""
     key = (op.n, op.nnz, op.pattern.n_groups, precision, op.vals64.device.index)
     hit = _tuned.get(key)
     if hit is not None:
@@ -316,10 +347,10 @@ def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", iters=24, b=Non
     rhs = torch.ones(op.n, dtype=torch.float64, device=dev) if b is None else b
     best, best_t = 16, float("inf")
     for lpg in LANES_PER_GROUP:
-        pcg_solve(op, rhs, tol=0.0, maxiter=4, precision=precision, lanes_per_group=lpg)   # load the kernels
+        pcg_solve(op, rhs, tol=0.0, maxiter=4, precision=precision, lanes_per_group=lpg, layout="csr")   # load
         a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        pcg_solve(op, rhs, tol=0.0, maxiter=iters, precision=precision, lanes_per_group=lpg, chunk=8)
+        pcg_solve(op, rhs, tol=0.0, maxiter=iters, precision=precision, lanes_per_group=lpg, chunk=8, layout="csr")
         e.record()
         e.synchronize()
         t = a.elapsed_time(e)
@@ -329,10 +360,16 @@ def tuned_lanes_per_group(op: ReducedOperator, precision="fp64", iters=24, b=Non
     return best
 
 
+LAYOUTS = ("sell", "csr")
+
+
 def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision="fp64", use_dinv=True,
-              reliable_delta=0.1, chunk=16, out=None, workspace=None, lanes_per_group=None):
+              reliable_delta=0.1, chunk=16, out=None, workspace=None, lanes_per_group=None, layout="sell"):
     """Jacobi-PCG on the device.  Returns (x, SolveInfo); the caller decides how to treat a
-    non-OK status (see ``raise_for``)."""
+    non-OK status (see ``raise_for``).  ``layout`` picks the SpMV operator for "fp64": the
+    sliced SELL-32 copy of K ("sell", built on first use; a K without node row groups, such as
+    a host SciPy matrix, falls back to its CSR) or the CSR itself ("csr"); "mixed" always runs
+    on its sliced 48-bit difference-form operator and "fp32" on the CSR."""
     if precision not in PRECISIONS:
         raise ValueError(f"precision must be one of {sorted(PRECISIONS)}, got {precision!r}")
     prec = PRECISIONS[precision]
@@ -351,14 +388,18 @@ def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision
         workspace = torch.empty(wbytes, dtype=torch.uint8, device=dev)
     if precision == "fp32" and op.vals32 is None:
         raise ValueError("fp32 precision needs the FP32 copy of K (assemble with want32=True)")
-    diff = C.byref(op.diff_operator()) if precision == "mixed" else None
+    if layout not in LAYOUTS:
+        raise ValueError(f"layout must be one of {LAYOUTS}, got {layout!r}")
+    grouped = op.pattern.group_ptr is not None and op.pattern.free_map.numel() > 0
+    use_sell = precision == "mixed" or (precision == "fp64" and layout == "sell" and grouped)
+    sell = C.byref(op.sell_operator(precision)) if use_sell else None
     csr = op.csr_struct()
     if lanes_per_group is None:
-        lanes_per_group = tuned_lanes_per_group(op, precision)
+        lanes_per_group = 8 if use_sell else tuned_lanes_per_group(op, precision)
     params = L.PcgParams(float(tol), int(maxiter or 0), prec, float(reliable_delta), int(chunk), 1 if use_dinv else 0,
                          int(lanes_per_group), 0)
     res = L.PcgResult()
-    rc = L.lib.feab_pcg_solve(C.byref(csr), diff, L.dptr(op.dinv64), L.dptr(op.dinv32), L.dptr(b), L.dptr(x0), L.dptr(x),
+    rc = L.lib.feab_pcg_solve(C.byref(csr), sell, L.dptr(op.dinv64), L.dptr(op.dinv32), L.dptr(b), L.dptr(x0), L.dptr(x),
                               C.byref(params), L.dptr(workspace), wbytes, C.byref(res), L.stream_ptr(dev))
     if rc in (L.FEAB_BAD_ARG, L.FEAB_CUDA_ERROR) and res.status == 0:
         res.status = rc
@@ -366,15 +407,28 @@ def pcg_solve(op: ReducedOperator, b, x0=None, tol=1e-8, maxiter=None, precision
                         float(res.bnorm), precision, int(res.graph_launches))
 
 
+def sell_spmv(op: ReducedOperator, x, precision="fp64", out=None):
+    """y = K_ff x through the sliced operator ("fp64" or "mixed" values)."""
+    x = torch.as_tensor(x).to(device=op.vals64.device, dtype=torch.float64).contiguous()
+    y = out if out is not None else torch.empty(op.n, dtype=torch.float64, device=op.vals64.device)
+    sell = op.sell_operator(precision)
+    csr = op.csr_struct()
+    rc = L.lib.feab_sell_spmv(C.byref(csr), C.byref(sell), L.dptr(x), L.dptr(y), L.stream_ptr(op.vals64.device))
+    L.raise_for(rc, "sliced spmv")
+    return y
+
+
 def spmv(op: ReducedOperator, x, precision="fp64", out=None, lanes_per_group=None):
-    """y = K_ff x with the PCG's SpMV kernel (FP64 or FP32 values)."""
+    """y = K_ff x with the CSR SpMV kernel of the PCG (FP64 or FP32 values); "mixed" runs the
+    sliced difference-form product."""
+    if precision == "mixed":
+        return sell_spmv(op, x, "mixed", out=out)
     prec = PRECISIONS[precision]
     dt = torch.float32 if precision == "fp32" else torch.float64
     x = torch.as_tensor(x).to(device=op.vals64.device, dtype=dt).contiguous()
     y = out if out is not None else torch.empty(op.n, dtype=dt, device=op.vals64.device)
     csr = op.csr_struct()
-    diff = C.byref(op.diff_operator()) if precision == "mixed" else None
     lpg = lanes_per_group if lanes_per_group is not None else tuned_lanes_per_group(op, precision)
-    rc = L.lib.feab_csr_spmv(C.byref(csr), diff, prec, int(lpg), L.dptr(x), L.dptr(y), L.stream_ptr(op.vals64.device))
+    rc = L.lib.feab_csr_spmv(C.byref(csr), None, prec, int(lpg), L.dptr(x), L.dptr(y), L.stream_ptr(op.vals64.device))
     L.raise_for(rc, "csr spmv")
     return y

@@ -86,6 +86,30 @@ typedef struct feab_diff_operator {
   int32_t* voff;     /* n_groups + 1: first value of each group             */
 } feab_diff_operator;
 
+/* Sliced (SELL-32) node-group operator for the single-right-hand-side PCG, built from the CSR
+ * by feab_sell_operator_build into caller storage (feab_sell_operator_bytes).  Node row groups
+ * are cut into slices of 32; lane l of a warp owns group 32 s + l, and slice s holds W_s column
+ * steps (a multiple of 4) from step soff[s].  Steps come in blocks of 4; for the block starting
+ * at step b, lane l's 4 columns are tcol[b * 32 + 4 l + u] and its row-k values are at
+ * (3 b + 4 k) * 32 + 4 l + u (u = 0..3), so each lane reads 16 contiguous bytes per load and
+ * each warp 512 contiguous bytes.
+ *   kind FEAB_PREC_FP64:  v64 holds the FP64 values; all columns (plain y = K x).
+ *   kind FEAB_PREC_MIXED: vhi/vlo hold the values rounded to 36 mantissa bits; own-node columns
+ *                         are left out and K is applied in difference form with the row-block
+ *                         sums S (as feab_diff_operator); tcol carries the DOF component.
+ * Steps past a group's length point at the node's own first free DOF with value 0. */
+typedef struct feab_sell_operator {
+  int32_t kind;      /* FEAB_PREC_FP64 or FEAB_PREC_MIXED                       */
+  int32_t n_slices;  /* ceil(n_groups / 32)                                     */
+  int32_t* soff;     /* n_slices + 1: first column step of each slice           */
+  int32_t* tcol;     /* 32 per step                                             */
+  double* v64;       /* FP64 kind: 96 per step                                  */
+  uint32_t* vhi;     /* MIXED kind: 96 per step                                 */
+  uint16_t* vlo;     /* MIXED kind: 96 per step                                 */
+  uint8_t* gmask;    /* MIXED kind: n_groups free-DOF masks                     */
+  double* S;         /* MIXED kind: 3 n row-block sums                          */
+} feab_sell_operator;
+
 typedef struct feab_pcg_params {
   double tol;                /* on ||b - A x|| / ||b||  (||b|| := 1 when b == 0)          */
   int32_t maxiter;           /* <= 0: 10 n, as iterative_solvers.py:393-394              */
@@ -185,12 +209,15 @@ int32_t feab_hex8_apply(const double* ke_packed, const int32_t* conn, const int3
 /* ---------------------------------------------------------------- PCG
  * Jacobi-preconditioned CG, the recurrence of preconditioned_cg
  * (iterative_solvers.py:362-481) and _cg_torch (torch_sparse_solver.py:165-202).
- * FEAB_PREC_FP64 follows the reference step for step in FP64.  The other precisions declare
- * convergence only on an FP64 residual b - K x computed with the FP64 values.
+ * FEAB_PREC_FP64 follows the reference step for step in FP64, through the CSR or, when `sell`
+ * (kind FEAB_PREC_FP64) is given, through the sliced operator.  FEAB_PREC_MIXED needs `sell` of
+ * kind FEAB_PREC_MIXED; FEAB_PREC_FP32 uses the CSR's vals32.  The precisions other than FP64
+ * declare convergence only on an FP64 residual b - K x computed with the FP64 values.
  * Synchronous: returns when the solve has finished; *result holds the outcome. */
 size_t feab_pcg_workspace_bytes(int32_t n, int32_t precision);
 
-/* Upper bound from the sizes alone (no device work); needs nnz + 3 n_groups < 2^31. */
+/* Difference-form operator for the batched block-PCG (feab_block_pcg_solve); upper bound from
+ * the sizes alone (no device work); needs nnz + 3 n_groups < 2^31. */
 size_t feab_diff_operator_bytes(int32_t n, int64_t nnz, int32_t n_groups);
 
 /* dof_of[r] = original DOF of reduced row r (free_dofs, solver.py:1400-1401).  A needs
@@ -198,7 +225,7 @@ size_t feab_diff_operator_bytes(int32_t n, int64_t nnz, int32_t n_groups);
 int32_t feab_diff_operator_build(const feab_csr* A, const int32_t* dof_of, void* storage, size_t storage_bytes,
                                  feab_diff_operator* out, cudaStream_t stream);
 
-int32_t feab_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const double* dinv64,
+int32_t feab_pcg_solve(const feab_csr* A, const feab_sell_operator* sell, const double* dinv64,
                        const float* dinv32, const double* b, const double* x0, double* x,
                        const feab_pcg_params* params, void* workspace, size_t workspace_bytes,
                        feab_pcg_result* result, cudaStream_t stream);
@@ -225,12 +252,27 @@ int32_t feab_pcg_solve_noalloc(const feab_csr* A, const double* dinv64, const do
                                double* x, const feab_pcg_params* params, feab_pcg_result* result,
                                cudaStream_t stream);
 
+/* Storage for a sliced operator of the CSR A (n rows, n_groups node groups) whose longest row has
+ * max_row_len entries (81 for hex8 meshes). */
+size_t feab_sell_operator_bytes(int32_t n, int32_t n_groups, int32_t max_row_len, int32_t kind);
+
+/* Builds the sliced operator (A needs group_ptr; dof_of as for feab_diff_operator_build, only
+ * read for the MIXED kind).  FEAB_BAD_ARG if a row is longer than max_row_len.  Synchronous. */
+int32_t feab_sell_operator_build(const feab_csr* A, const int32_t* dof_of, int32_t kind, int32_t max_row_len,
+                                 void* storage, size_t storage_bytes, feab_sell_operator* out, cudaStream_t stream);
+
+/* y = A x (x, y double) through the sliced operator: the same product as the CSR SpMV
+ * `A @ p` of preconditioned_cg (iterative_solvers.py:448), in FP64 or the mixed difference form. */
+int32_t feab_sell_spmv(const feab_csr* A, const feab_sell_operator* op, const double* x, double* y,
+                       cudaStream_t stream);
+
 /* y = A x with the PCG's SpMV kernel (same code and launch shape as one PCG step's SpMV).
  * FEAB_PREC_FP64: x, y double, vals64; FEAB_PREC_FP32: x, y float, vals32;
- * FEAB_PREC_MIXED: x, y double, difference form (diff != NULL).
+ * FEAB_PREC_MIXED: x, y double, difference form through a MIXED sliced operator (sell);
+ * FEAB_PREC_FP64 with an FP64 sliced operator: the sliced product instead of the CSR one.
  * Replaces the CSR SpMV `A @ p` of preconditioned_cg (iterative_solvers.py:448) /
  * `K_t @ x` of torch_sparse_cg_solve (torch_sparse_solver.py:255-256). */
-int32_t feab_csr_spmv(const feab_csr* A, const feab_diff_operator* diff, int32_t precision, int32_t lanes_per_group,
+int32_t feab_csr_spmv(const feab_csr* A, const feab_sell_operator* sell, int32_t precision, int32_t lanes_per_group,
                       const void* x, void* y, cudaStream_t stream);
 
 /* ---------------------------------------------------------------- batched multi-RHS PCG

@@ -46,7 +46,8 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spmv-reps", type=int, default=20)
-    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram"], default="cantilever",
+    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv"],
+                    default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
     return ap.parse_args()
@@ -103,6 +104,18 @@ class ClockSampler:
                                          stderr=subprocess.DEVNULL)
         except (OSError, ValueError):
             self.proc = None
+
+    def wait_first_sample(self, timeout=20.0):
+        """nvidia-smi's start-up can stall the GPU for a moment: wait until it has written its
+        first sample, so that this happens before a timed region, not inside it."""
+        if self.proc is None:
+            return
+        t0 = time.time()
+        while time.time() - t0 < timeout and self.proc.poll() is None:
+            self.out.flush()
+            if os.path.getsize(self.path) > 0:
+                return
+            time.sleep(0.05)
 
     def stop(self):
         if self.proc is None:
@@ -176,10 +189,12 @@ def time_steps(prob, precision, tol, steps, warmup, world):
     barrier(world)
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n0 = L.lib.feab_launch_count()
+    torch.cuda.nvtx.range_push(f"feab_timed_{precision}")     # lets a profiler select the timed steps
     start.record()
     for _ in range(steps):
         x, dc, info, op = prob.step(precision, tol)
     end.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     launches = int(L.lib.feab_launch_count() - n0)
     ms = start.elapsed_time(end) / steps
@@ -241,14 +256,14 @@ def spmv_bytes(op, precision):
 def spmv_roofline(op, precision, reps, peak_gbs):
     """Average duration of the PCG's SpMV kernel (the sliced SELL-32 product for fp64 and mixed,
     the CSR one for fp32) with CUDA events on the launching stream; L2 is flushed before each
-    launch by a 256 MB write."""
+    launch (L2Flush: a 256 MB write, then a 256 MB read)."""
     import torch
     from feab200.device import sell_spmv, spmv, tuned_lanes_per_group
     dev = op.vals64.device
     dt = torch.float32 if precision == "fp32" else torch.float64
     x = torch.randn(op.n, dtype=dt, device=dev)
     y = torch.empty(op.n, dtype=dt, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    flush = L2Flush(dev)
     if precision == "fp32":
         lpg = tuned_lanes_per_group(op, precision)
         run = lambda: spmv(op, x, precision, out=y, lanes_per_group=lpg)  # noqa: E731
@@ -258,7 +273,7 @@ def spmv_roofline(op, precision, reps, peak_gbs):
     run()
     times = []
     for _ in range(reps):
-        flush.fill_(1.0)
+        flush()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         run()
@@ -276,6 +291,23 @@ def spmv_roofline(op, precision, reps, peak_gbs):
             "kernel": f"{kern} (the SpMV of PCG step A, {precision})",
             "bytes_per_launch": int(nbytes),
             "csr_formula_bytes": int(bytes_csr), "launch_us": round(t * 1e6, 2)}
+
+
+class L2Flush:
+    """Evicts L2 before a timed launch: writes one 256 MB buffer (twice the 126 MB L2), then reads
+    a second one, so that the dirty lines of the write are written back before the timed kernel
+    starts and L2 holds only clean, unrelated lines."""
+
+    def __init__(self, device):
+        import torch
+        self.w = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+        self.r = torch.ones(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+        self.sink = torch.empty(1, dtype=torch.float32, device=device)
+
+    def __call__(self):
+        import torch
+        self.w.fill_(1.0)
+        torch.sum(self.r, dim=0, keepdim=True, out=self.sink)
 
 
 def measured_peak():
@@ -482,12 +514,12 @@ def workload_gram(args):
     n, k = 1_382_976, 64
     g = torch.Generator(device="cuda").manual_seed(5)
     X = torch.randn((n, k), generator=g, device="cuda", dtype=torch.float32)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    flush = L2Flush("cuda")
     for _ in range(args.warmup):
         gram_bf16x3(X)
     times = []
     for _ in range(args.steps):
-        flush.fill_(1.0)
+        flush()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
         G = gram_bf16x3(X)
@@ -507,6 +539,32 @@ def workload_gram(args):
             "gram_rel_err_vs_fp64": err, "lambda_max": float(w[0])}
 
 
+def workload_spmv(args):
+    """The PCG's SpMV kernels alone on the 128x32x32 cantilever's K_ff (inputs resident, L2
+    flushed before each timed launch): the sliced operator with FP64 and 48-bit values, and the
+    CSR kernel; a few PCG iterations of each precision run first, so that a profiler sees the
+    step kernels early."""
+    import torch
+    from feab200.device import DeviceMesh, pcg_solve
+    c = build_workload(tuple(args.shape))
+    dm = DeviceMesh(c.mesh.nodes, c.mesh.elements)
+    op = dm.assemble(dm.element_stiffness(c.D), dm.pattern(c.fixed), want32=True)
+    peak, kind = measured_peak()
+    b = torch.as_tensor(c.F[c.free]).to(op.vals64.device)
+    iters = {}
+    for prec in ("mixed", "fp64"):
+        _, info = pcg_solve(op, b, tol=0.0, maxiter=8, precision=prec)
+        iters[prec] = info.iters
+    out = {}
+    for prec in ("mixed", "fp64", "fp32"):
+        r = spmv_roofline(op, prec, max(1, args.steps), peak)
+        r["peak_source"] = f"MEASURED_PEAKS.json hbm_gbs (of {kind})"
+        out[prec] = r
+    return {"metric": "PCG SpMV kernel time, 128x32x32 K_ff (n 418176, nnz 32348142), mixed 48-bit sliced",
+            "value": out["mixed"]["launch_us"], "unit": "us", "roofline": out["mixed"],
+            "roofline_fp64": out["fp64"], "roofline_fp32_csr": out["fp32"], "pcg_probe_iters": iters}
+
+
 # ----------------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -515,7 +573,7 @@ def main():
     args.world, args.rank = world, rank
     if args.workload != "cantilever" and args.impl == "ours":
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
-              "gram": workload_gram}[args.workload]
+              "gram": workload_gram, "spmv": workload_spmv}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})
@@ -554,6 +612,7 @@ def main():
     clocks = ClockSampler(gpu_index(local))
     # plain FP64 first, then mixed (the headline)
     clocks.start()
+    clocks.wait_first_sample()
     ms64, x64, dc64, info64, op64, _ = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
     ms32, x32, dc32, info32, op, launches = time_steps(prob, "mixed", args.tol, args.steps, args.warmup, world)
     clk = clocks.stop()

@@ -57,6 +57,7 @@ struct PcgArgs {
   const float* vals32;
   SellView sell;           // sliced operator (FP64 or mixed values), when use_sell
   int use_sell;
+  int vec2;                // x and dinv64 16-byte aligned: the vector passes use double2
   const double* dinv64;
   const float* dinv32;
   const double* b;
@@ -390,14 +391,24 @@ __global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
   const PcgState* S = A.S_;
   if (S->done || !S->p_pending) return;
   const double beta = S->beta;
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += gridDim.x * blockDim.x)
-    A.p0[i] = A.z[i] + beta * A.p0[i];
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x, stride = gridDim.x * blockDim.x;
+  if (!A.vec2) {
+    for (int i = t0; i < A.n; i += stride) A.p0[i] = A.z[i] + beta * A.p0[i];
+    return;
+  }
+  double2* __restrict__ p2 = reinterpret_cast<double2*>(A.p0);
+  const double2* __restrict__ z2 = reinterpret_cast<const double2*>(A.z);
+  for (int i = t0; i < (A.n >> 1); i += stride) {
+    const double2 pv = p2[i], zv = z2[i];
+    p2[i] = make_double2(zv.x + beta * pv.x, zv.y + beta * pv.y);
+  }
+  if ((A.n & 1) && t0 == 0) A.p0[A.n - 1] = A.z[A.n - 1] + beta * A.p0[A.n - 1];
 }
 
 // Sliced path, kernel A: Ap = K p and p.Ap through the SELL-32 operator (PREC = its kind); in a
 // mixed reliable step, the FP64 residual r = b - K64 x through the CSR values instead.
 template <int PREC>
-__global__ void __launch_bounds__(kThreads, 4) k_step_a_sell(PcgArgs A) {
+__global__ void __launch_bounds__(kThreads, FEAB_SELL_MINB) k_step_a_sell(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
@@ -488,7 +499,8 @@ __global__ void __launch_bounds__(kThreads) k_step_b(PcgArgs A) {
   } else {
     const double alpha = S->alpha;
     const double* __restrict__ p = psel ? A.p1 : A.p0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < A.n; i += stride) {
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    auto one = [&](int i) {
       A.x[i] += alpha * p[i];
       const double ri = A.r[i] - alpha * A.Ap[i];
       A.r[i] = ri;
@@ -496,6 +508,31 @@ __global__ void __launch_bounds__(kThreads) k_step_b(PcgArgs A) {
       A.z[i] = zi;
       part[0] += ri * ri;
       part[1] += ri * zi;
+    };
+    if (A.vec2) {
+      // two rows per thread with 16-byte loads, all loads of the pair issued together
+      const double2* __restrict__ p2 = reinterpret_cast<const double2*>(p);
+      double2* __restrict__ x2 = reinterpret_cast<double2*>(A.x);
+      double2* __restrict__ r2 = reinterpret_cast<double2*>(A.r);
+      double2* __restrict__ z2 = reinterpret_cast<double2*>(A.z);
+      const double2* __restrict__ a2 = reinterpret_cast<const double2*>(A.Ap);
+      const double2* __restrict__ d2 = reinterpret_cast<const double2*>(A.dinv64);
+      for (int i = t0; i < (A.n >> 1); i += stride) {
+        const double2 pv = p2[i], xv = x2[i], rv = r2[i], av = a2[i];
+        const double2 dv = A.use_dinv ? d2[i] : make_double2(1.0, 1.0);
+        const double r0 = rv.x - alpha * av.x, r1 = rv.y - alpha * av.y;
+        const double z0 = A.use_dinv ? dv.x * r0 : r0, z1 = A.use_dinv ? dv.y * r1 : r1;
+        x2[i] = make_double2(xv.x + alpha * pv.x, xv.y + alpha * pv.y);
+        r2[i] = make_double2(r0, r1);
+        z2[i] = make_double2(z0, z1);
+        part[0] += r0 * r0;
+        part[0] += r1 * r1;
+        part[1] += r0 * z0;
+        part[1] += r1 * z1;
+      }
+      if ((A.n & 1) && t0 == 0) one(A.n - 1);
+    } else {
+      for (int i = t0; i < A.n; i += stride) one(i);
     }
   }
   double tot[2];
@@ -666,7 +703,7 @@ Grids grids_for(int n, int G) {
   Grids g;
   // A: one warp per tile of 32 groups, 8 warps per block
   g.a = std::max(1, (int)std::min<int64_t>(((int64_t)G + 255) / 256, (int64_t)max_grid()));
-  g.b = std::max(1, (int)std::min<int64_t>(((int64_t)n + kThreads * 4 - 1) / (kThreads * 4), (int64_t)max_grid()));
+  g.b = std::max(1, (int)std::min<int64_t>(((int64_t)n + kThreads * 2 - 1) / (kThreads * 2), (int64_t)max_grid()));
   return g;
 }
 
@@ -855,6 +892,14 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
   return st;
 }
 
+// The FP64 vector passes read two rows per 16-byte load when every vector they touch is 16-byte
+// aligned (workspace vectors sit at 256-byte offsets of the caller's buffer).
+void set_vec2(PcgArgs* A) {
+  auto al = [](const void* p) { return p == nullptr || (reinterpret_cast<uintptr_t>(p) & 15u) == 0; };
+  A->vec2 = al(A->x) && (!A->use_dinv || al(A->dinv64)) && al(A->r) && al(A->z) && al(A->p0) && al(A->p1) &&
+            al(A->Ap);
+}
+
 void fill_matrix(const feab_csr* M, PcgArgs* A) {
   A->n = M->n;
   A->n_groups = M->n_groups;
@@ -987,6 +1032,7 @@ extern "C" int32_t feab_pcg_solve(const feab_csr* M, const feab_sell_operator* s
   A.x0 = x0;
   A.x = x;
   A.use_dinv = prm->use_dinv ? 1 : 0;
+  set_vec2(&A);
   const int maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
   const double delta = prm->reliable_delta > 0.0 && prm->reliable_delta < 1.0 ? prm->reliable_delta : 0.1;
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
@@ -1098,6 +1144,7 @@ extern "C" int32_t feab_pcg_solve_noalloc(const feab_csr* M, const double* dinv6
   A.x0 = x0;
   A.x = x;
   A.use_dinv = prm->use_dinv ? 1 : 0;
+  set_vec2(&A);
   const int maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
   const int lpg = normalize_lpg(prm->lanes_per_group);

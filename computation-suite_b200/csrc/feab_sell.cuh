@@ -15,7 +15,38 @@
 #pragma once
 #include "feab_common.cuh"
 
+// Blocks of 4 steps that a warp asks L2 to fetch ahead of its loads (0: none).
+#ifndef FEAB_SELL_PREFETCH
+#define FEAB_SELL_PREFETCH 0
+#endif
+// Blocks of 4 steps whose loads a lane issues before it consumes any.
+#ifndef FEAB_SELL_BLOCKS
+#define FEAB_SELL_BLOCKS 2
+#endif
+// 1: load the operator with the streaming (evict-first) cache hint, so that the CG vectors
+// (a few MB, re-read every iteration) stay in L2 while K streams through it.
+#ifndef FEAB_SELL_STREAM
+#define FEAB_SELL_STREAM 1
+#endif
+// Minimum resident 256-thread CTAs per SM for the sliced SpMV kernels (register budget).
+#ifndef FEAB_SELL_MINB
+#define FEAB_SELL_MINB 2
+#endif
+
 namespace feab {
+
+template <typename T>
+__device__ __forceinline__ T ld_op(const T* p) {
+#if FEAB_SELL_STREAM
+  return __ldcs(p);
+#else
+  return __ldg(p);
+#endif
+}
+
+__device__ __forceinline__ void prefetch_l2(const void* p, unsigned bytes) {
+  asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(bytes) : "memory");
+}
 
 struct SellView {
   int kind;                 // FEAB_PREC_FP64: plain y = K x; FEAB_PREC_MIXED: difference form
@@ -61,55 +92,91 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
   for (int j = 0; j < 3; ++j)
     xs[j] = (KIND == FEAB_PREC_MIXED && L.valid && ((L.mask >> j) & 1)) ? xf(L.r0 + __popc(L.mask & ((1 << j) - 1)))
                                                                        : 0.0;
-  for (int j = 0; j < W; j += 4) {
-    const size_t b = (size_t)(base + j);
-    const uint4 tq = __ldg(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
-    const unsigned t[4] = {tq.x, tq.y, tq.z, tq.w};
-    if (KIND == FEAB_PREC_FP64) {
-      double v[3][4];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const double2* vp = reinterpret_cast<const double2*>(V.v64 + (3 * b + 4 * k) * 32) + 2 * lane;
-        const double2 p0 = __ldg(vp), p1 = __ldg(vp + 1);
-        v[k][0] = p0.x;
-        v[k][1] = p0.y;
-        v[k][2] = p1.x;
-        v[k][3] = p1.y;
+  // one lane asks L2 for the blocks FEAB_SELL_PREFETCH ahead (16-byte aligned, sizes multiple of
+  // 16, never past the slice's last block)
+  auto prefetch_block = [&](int jj) {
+    if (FEAB_SELL_PREFETCH > 0 && lane == 0 && jj < W) {
+      const size_t b2 = (size_t)(base + jj);
+      prefetch_l2(V.tcol + b2 * 32, 512u);
+      if (KIND == FEAB_PREC_FP64) {
+        prefetch_l2(V.v64 + 3 * b2 * 32, 3072u);
+      } else {
+        prefetch_l2(V.vhi + 3 * b2 * 32, 1536u);
+        prefetch_l2(V.vlo + 3 * b2 * 32, 768u);
       }
+    }
+  };
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const double xv = xf((int)t[u]);
-        a0 = fma(v[0][u], xv, a0);
-        a1 = fma(v[1][u], xv, a1);
-        a2 = fma(v[2][u], xv, a2);
-      }
-    } else {
-      uint4 h[3];
-      uint2 l[3];
+  for (int i = 1; i < FEAB_SELL_PREFETCH; ++i) prefetch_block(4 * i);
+  for (int j = 0; j < W; j += 4 * FEAB_SELL_BLOCKS) {
+    prefetch_block(j + 4 * FEAB_SELL_PREFETCH);
+    // all loads of FEAB_SELL_BLOCKS blocks first (a block past the slice end is skipped; W is
+    // the same for the whole warp, so the test does not diverge)
+    unsigned t[FEAB_SELL_BLOCKS][4];
+    double v[KIND == FEAB_PREC_FP64 ? FEAB_SELL_BLOCKS : 1][3][4];
+    uint4 h[KIND == FEAB_PREC_FP64 ? 1 : FEAB_SELL_BLOCKS][3];
+    uint2 l[KIND == FEAB_PREC_FP64 ? 1 : FEAB_SELL_BLOCKS][3];
 #pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        const size_t o = (3 * b + 4 * k) * 32;
-        h[k] = __ldg(reinterpret_cast<const uint4*>(V.vhi + o) + lane);
-        l[k] = __ldg(reinterpret_cast<const uint2*>(V.vlo + o) + lane);
-      }
-      double d[4];
+    for (int nb = 0; nb < FEAB_SELL_BLOCKS; ++nb) {
+      if (nb > 0 && j + 4 * nb >= W) break;
+      const size_t b = (size_t)(base + j + 4 * nb);
+      const uint4 tq = ld_op(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
+      t[nb][0] = tq.x;
+      t[nb][1] = tq.y;
+      t[nb][2] = tq.z;
+      t[nb][3] = tq.w;
+      if (KIND == FEAB_PREC_FP64) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const unsigned jc = t[u] >> 30;
-        d[u] = xf((int)(t[u] & 0x3fffffffu)) - (jc == 0u ? xs[0] : (jc == 1u ? xs[1] : xs[2]));
+        for (int k = 0; k < 3; ++k) {
+          const double2* vp = reinterpret_cast<const double2*>(V.v64 + (3 * b + 4 * k) * 32) + 2 * lane;
+          const double2 p0 = ld_op(vp), p1 = ld_op(vp + 1);
+          v[nb][k][0] = p0.x;
+          v[nb][k][1] = p0.y;
+          v[nb][k][2] = p1.x;
+          v[nb][k][3] = p1.y;
+        }
+      } else {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          const size_t o = (3 * b + 4 * k) * 32;
+          h[nb][k] = ld_op(reinterpret_cast<const uint4*>(V.vhi + o) + lane);
+          l[nb][k] = ld_op(reinterpret_cast<const uint2*>(V.vlo + o) + lane);
+        }
       }
-      a0 = fma(sell_dec48(h[0].x, (uint16_t)(l[0].x & 0xffffu)), d[0], a0);
-      a0 = fma(sell_dec48(h[0].y, (uint16_t)(l[0].x >> 16)), d[1], a0);
-      a0 = fma(sell_dec48(h[0].z, (uint16_t)(l[0].y & 0xffffu)), d[2], a0);
-      a0 = fma(sell_dec48(h[0].w, (uint16_t)(l[0].y >> 16)), d[3], a0);
-      a1 = fma(sell_dec48(h[1].x, (uint16_t)(l[1].x & 0xffffu)), d[0], a1);
-      a1 = fma(sell_dec48(h[1].y, (uint16_t)(l[1].x >> 16)), d[1], a1);
-      a1 = fma(sell_dec48(h[1].z, (uint16_t)(l[1].y & 0xffffu)), d[2], a1);
-      a1 = fma(sell_dec48(h[1].w, (uint16_t)(l[1].y >> 16)), d[3], a1);
-      a2 = fma(sell_dec48(h[2].x, (uint16_t)(l[2].x & 0xffffu)), d[0], a2);
-      a2 = fma(sell_dec48(h[2].y, (uint16_t)(l[2].x >> 16)), d[1], a2);
-      a2 = fma(sell_dec48(h[2].z, (uint16_t)(l[2].y & 0xffffu)), d[2], a2);
-      a2 = fma(sell_dec48(h[2].w, (uint16_t)(l[2].y >> 16)), d[3], a2);
+    }
+#pragma unroll
+    for (int nb = 0; nb < FEAB_SELL_BLOCKS; ++nb) {
+      if (nb > 0 && j + 4 * nb >= W) break;
+      if (KIND == FEAB_PREC_FP64) {
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const double xv = xf((int)t[nb][u]);
+          a0 = fma(v[nb][0][u], xv, a0);
+          a1 = fma(v[nb][1][u], xv, a1);
+          a2 = fma(v[nb][2][u], xv, a2);
+        }
+      } else {
+        double d[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const unsigned jc = t[nb][u] >> 30;
+          d[u] = xf((int)(t[nb][u] & 0x3fffffffu)) - (jc == 0u ? xs[0] : (jc == 1u ? xs[1] : xs[2]));
+        }
+        const uint4* hh = h[nb];
+        const uint2* ll = l[nb];
+        a0 = fma(sell_dec48(hh[0].x, (uint16_t)(ll[0].x & 0xffffu)), d[0], a0);
+        a0 = fma(sell_dec48(hh[0].y, (uint16_t)(ll[0].x >> 16)), d[1], a0);
+        a0 = fma(sell_dec48(hh[0].z, (uint16_t)(ll[0].y & 0xffffu)), d[2], a0);
+        a0 = fma(sell_dec48(hh[0].w, (uint16_t)(ll[0].y >> 16)), d[3], a0);
+        a1 = fma(sell_dec48(hh[1].x, (uint16_t)(ll[1].x & 0xffffu)), d[0], a1);
+        a1 = fma(sell_dec48(hh[1].y, (uint16_t)(ll[1].x >> 16)), d[1], a1);
+        a1 = fma(sell_dec48(hh[1].z, (uint16_t)(ll[1].y & 0xffffu)), d[2], a1);
+        a1 = fma(sell_dec48(hh[1].w, (uint16_t)(ll[1].y >> 16)), d[3], a1);
+        a2 = fma(sell_dec48(hh[2].x, (uint16_t)(ll[2].x & 0xffffu)), d[0], a2);
+        a2 = fma(sell_dec48(hh[2].y, (uint16_t)(ll[2].x >> 16)), d[1], a2);
+        a2 = fma(sell_dec48(hh[2].z, (uint16_t)(ll[2].y & 0xffffu)), d[2], a2);
+        a2 = fma(sell_dec48(hh[2].w, (uint16_t)(ll[2].y >> 16)), d[3], a2);
+      }
     }
   }
   if (KIND == FEAB_PREC_MIXED) {

@@ -5,6 +5,10 @@
 // (batched_solve.py:105-164) applies one factorisation to many columns -- while the matrix is
 // read once per step for all columns of a problem (SpMM over the panel).
 //
+// One step is three kernels: P (P = Z + beta P for problems with a pending direction), A (SpMM
+// AP = K P and the per-column p.Ap, or the FP64 residual in a reliable step) and B (X, R, Z,
+// per-column r.r and r.z, convergence, beta).
+//
 // Layout: vectors are row-major panels n x K (K = panel width, a power of two <= 64);
 // problem p owns a contiguous row range and a contiguous range of node row groups.  Work is
 // cut into items of <= 64 groups of one problem; a block processes items (grid-stride), and
@@ -30,9 +34,13 @@ constexpr int kModeCG = 0;
 constexpr int kModeReliable = 1;
 
 struct ProbState {  // per problem
-  int32_t mode, pending, psel, done, status, iters, reliable;
+  int32_t mode, pending, psel, done, status, iters, reliable, last_reliable;
   uint32_t ticket_a, ticket_b;
 };
+
+// Mixed: fewest CG steps between two FP64 residual replacements of a problem, unless every
+// unconverged column is ready for one (a replacement is an FP64 SpMM over the whole panel).
+constexpr int kMinReliableGap = 32;
 
 struct ColState {  // per (problem, column)
   double bnorm, rz_old, rz_prev, alpha, beta, rr, relres, rmax;
@@ -60,7 +68,7 @@ struct BArgs {
   const int32_t* prob_cols;
   const double* B;   // n x k
   double* X;         // n x k
-  double *R, *Z, *P0, *P1, *AP;
+  double *R, *Z, *P0, *AP;
   double* part;      // n_items x 2k
   ProbState* ps;
   ColState* cs;
@@ -93,11 +101,44 @@ __device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
   return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
 }
 
-// SpMM for one row group: acc[row][.] for this lane's panel columns.
+// A warp's staging area for one row group's columns and values (FP64, decoded from the 48-bit
+// form for the difference operator), filled with coalesced loads before the SpMM reads them as
+// broadcasts; groups longer than kStageCols are staged in pieces.
+constexpr int kStageCols = 128;
+constexpr int kUnroll = 4;  // matrix columns whose panel rows a lane gathers before using any
+
+struct GroupStage {
+  int col[kStageCols];
+  double val[3][kStageCols];
+};
+
+// Panel column of accumulator q of lane-in-sub-warp cl: a 64-wide panel gives each lane two
+// adjacent columns (one 16-byte gather per panel row), narrower panels one column per lane.
+template <int K>
+__device__ __forceinline__ int panel_col(int cl, int q) {
+  return K >= 64 ? 2 * cl + q : cl + 32 * q;
+}
+
+// The lane's CPL values of panel row j of src (n x K, row major; 16-byte aligned when K = 64).
+template <int K>
+__device__ __forceinline__ void gather_row(const double* __restrict__ src, int j, int cl,
+                                           double (&v)[K >= 32 ? K / 32 : 1]) {
+  if constexpr (K >= 64) {
+    const double2 t = __ldg(reinterpret_cast<const double2*>(src + (int64_t)j * K) + cl);
+    v[0] = t.x;
+    v[1] = t.y;
+  } else {
+    v[0] = __ldg(src + (int64_t)j * K + cl);
+  }
+}
+
+// SpMM for one row group: acc[row][q] = (K src)[row][panel_col(cl, q)].
 // Lanes are split into MPW = max(1, 32/K) sub-warps, each walking every MPW-th matrix column;
-// a lane covers CPL = max(1, K/32) panel columns c = (lane % min(K,32)) + 32*q.
-template <int K, bool DIFF, typename PF>
-__device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF pf, double (&acc)[3][K >= 32 ? K / 32 : 1]) {
+// a lane covers CPL = max(1, K/32) panel columns.
+template <int K, bool DIFF>
+__device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, GroupStage& st,
+                                           const double* __restrict__ src,
+                                           double (&acc)[3][K >= 32 ? K / 32 : 1]) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int MPW = K >= 32 ? 1 : 32 / K;
   constexpr int LW = K >= 32 ? 32 : K;  // lanes per sub-warp
@@ -112,42 +153,65 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, PF p
 #pragma unroll
     for (int q = 0; q < CPL; ++q) acc[k][q] = 0.0;
   double xs[3][CPL];
-  int mask = 0;
   if (DIFF) {
-    mask = A.gmask[g];
+    const int mask = A.gmask[g];
 #pragma unroll
-    for (int j = 0; j < 3; ++j)
+    for (int j = 0; j < 3; ++j) {
+      if ((mask >> j) & 1) {
+        gather_row<K>(src, r0 + __popc(mask & ((1 << j) - 1)), cl, xs[j]);
+      } else {
 #pragma unroll
-      for (int q = 0; q < CPL; ++q)
-        xs[j][q] = ((mask >> j) & 1) ? pf(r0 + __popc(mask & ((1 << j) - 1)), cl + 32 * q, q) : 0.0;
-  }
-  for (int m = sub; m < len; m += MPW) {
-    if (!DIFF) {
-      const int j = __ldg(A.col_idx + s0 + m);
-      double w[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k) w[k] = k < f ? __ldg(A.vals64 + s0 + k * len + m) : 0.0;
-#pragma unroll
-      for (int q = 0; q < CPL; ++q) {
-        const double xv = pf(j, cl + 32 * q, q);
-#pragma unroll
-        for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * xv;
-      }
-    } else {
-      const unsigned t = (unsigned)__ldg(A.tcol + c0 + m);
-      const int j = (int)(t & 0x3fffffffu), jc = (int)(t >> 30);
-      if (j >= r0 && j < r0 + f) continue;  // padding (own node, value 0)
-      double w[3];
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-        w[k] = k < f ? dec48(__ldg(A.vhi + s0 + k * len + m), __ldg(A.vlo + s0 + k * len + m)) : 0.0;
-#pragma unroll
-      for (int q = 0; q < CPL; ++q) {
-        const double d = pf(j, cl + 32 * q, q) - (jc == 0 ? xs[0][q] : (jc == 1 ? xs[1][q] : xs[2][q]));
-#pragma unroll
-        for (int k = 0; k < 3; ++k) acc[k][q] += w[k] * d;
+        for (int q = 0; q < CPL; ++q) xs[j][q] = 0.0;
       }
     }
+  }
+  for (int cb = 0; cb < len; cb += kStageCols) {
+    const int nc = min(kStageCols, len - cb);
+    for (int m = lane; m < nc; m += 32) {
+      if (!DIFF) {
+        st.col[m] = __ldg(A.col_idx + s0 + cb + m);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) st.val[k][m] = k < f ? __ldg(A.vals64 + s0 + k * len + cb + m) : 0.0;
+      } else {
+        st.col[m] = __ldg(A.tcol + c0 + cb + m);
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+          st.val[k][m] = k < f ? dec48(__ldg(A.vhi + s0 + k * len + cb + m), __ldg(A.vlo + s0 + k * len + cb + m))
+                               : 0.0;
+      }
+    }
+    __syncwarp();
+    for (int m0 = sub; m0 < nc; m0 += MPW * kUnroll) {
+      unsigned t[kUnroll];
+      double xv[kUnroll][CPL];
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int m = m0 + u * MPW;
+        t[u] = m < nc ? (unsigned)st.col[m] : 0u;
+        if (m < nc) {
+          gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), cl, xv[u]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;
+        }
+      }
+#pragma unroll
+      for (int u = 0; u < kUnroll; ++u) {
+        const int m = m0 + u * MPW;
+        if (m >= nc) break;
+        const double w0 = st.val[0][m], w1 = st.val[1][m], w2 = st.val[2][m];
+        const unsigned jc = t[u] >> 30;
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) {
+          // difference form: padding columns carry value 0 and point at the own node (d = 0)
+          const double d = DIFF ? xv[u][q] - (jc == 0u ? xs[0][q] : (jc == 1u ? xs[1][q] : xs[2][q])) : xv[u][q];
+          acc[0][q] = fma(w0, d, acc[0][q]);
+          acc[1][q] = fma(w1, d, acc[1][q]);
+          acc[2][q] = fma(w2, d, acc[2][q]);
+        }
+      }
+    }
+    __syncwarp();
   }
   // combine the sub-warps (lanes with equal cl)
 #pragma unroll
@@ -229,6 +293,7 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
         P.psel = 0;
         P.iters = 0;
         P.reliable = 0;
+        P.last_reliable = 0;
         P.status = FEAB_OK;
         P.done = all;
         if (all) atomicSub(A.remaining, 1);
@@ -238,38 +303,28 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
   }
 }
 
-// Step A: P_new = Z + beta P_old on the fly; AP = K P_new (or, in a reliable step, R = B - K64 X);
+// Step A: AP = K P (P updated by k_bstep_p; or, in a reliable step, R = B - K64 X);
 // per-column partial p.Ap (or r.r).
 template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
   __shared__ double sm[kWarps][K];
+  __shared__ GroupStage stage[kWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
     const ProbState P = A.ps[p];
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
-    const double* po = P.psel ? A.P1 : A.P0;
-    double* pn = P.psel ? A.P0 : A.P1;
-    const int pend = P.pending;
-    double beta[CPL];
-#pragma unroll
-    for (int q = 0; q < CPL; ++q) beta[q] = A.cs[(int64_t)p * K + (lane % LW) + 32 * q].beta;
+    const double* __restrict__ po = A.P0;  // the direction, already updated by k_bstep_p
     double part[CPL];
 #pragma unroll
     for (int q = 0; q < CPL; ++q) part[q] = 0.0;
     for (int g = A.item_g0[it] + w; g < A.item_g1[it]; g += kWarps) {
       double acc[3][CPL];
-      if (reliable) {
-        group_spmm<K, false>(A, g, lane, [&](int j, int c, int) { return A.X[(int64_t)j * K + c]; }, acc);
-      } else if (pend) {
-        group_spmm<K, MIXED>(A, g, lane, [&](int j, int c, int q) {
-          return A.Z[(int64_t)j * K + c] + beta[q] * po[(int64_t)j * K + c]; }, acc);
-      } else {
-        group_spmm<K, MIXED>(A, g, lane, [&](int j, int c, int) { return po[(int64_t)j * K + c]; }, acc);
-      }
+      if (reliable) group_spmm<K, false>(A, g, lane, stage[w], A.X, acc);
+      else group_spmm<K, MIXED>(A, g, lane, stage[w], po, acc);
       if (lane < LW) {
         const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
 #pragma unroll
@@ -277,14 +332,13 @@ __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
           if (k >= f) break;
 #pragma unroll
           for (int q = 0; q < CPL; ++q) {
-            const int64_t idx = (int64_t)(r0 + k) * K + lane + 32 * q;
+            const int64_t idx = (int64_t)(r0 + k) * K + panel_col<K>(lane, q);
             if (reliable) {
               const double ri = A.B[idx] - acc[k][q];
               A.R[idx] = ri;
               part[q] += ri * ri;
             } else {
-              const double pv = pend ? A.Z[idx] + beta[q] * po[idx] : po[idx];
-              if (pend) pn[idx] = pv;
+              const double pv = po[idx];
               A.AP[idx] = acc[k][q];
               part[q] += pv * acc[k][q];
             }
@@ -294,7 +348,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
     }
     if (lane < LW) {
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) sm[w][lane + 32 * q] = part[q];
+      for (int q = 0; q < CPL; ++q) sm[w][panel_col<K>(lane, q)] = part[q];
     }
     __syncthreads();
     if (threadIdx.x < K) {
@@ -324,7 +378,6 @@ __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
         ProbState& Pm = A.ps[p];
         Pm.ticket_a = 0;
         if (!reliable) {
-          if (pend) Pm.psel ^= 1;
           Pm.pending = 0;
           if (Pm.status != FEAB_OK) {
             Pm.done = 1;
@@ -337,12 +390,43 @@ __global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
   }
 }
 
+// Direction update P = Z + beta P (in place, per column beta; frozen columns have beta = 0, so
+// P = Z) for the problems whose new direction is pending.
+template <int K>
+__global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
+  const int c = threadIdx.x % K;
+  double* __restrict__ P0 = A.P0;
+  const double* __restrict__ Z = A.Z;
+  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+    const int p = A.item_problem[it];
+    const ProbState P = A.ps[p];
+    if (P.done || !P.pending) continue;
+    const double beta = A.cs[(int64_t)p * K + c].beta;
+    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
+    const int64_t e0 = (int64_t)r0 * K + threadIdx.x, e1 = (int64_t)r1 * K;
+    for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
+      double zv[4], pv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = idx + (int64_t)u * kThreads;
+        zv[u] = e < e1 ? Z[e] : 0.0;
+        pv[u] = e < e1 ? P0[e] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = idx + (int64_t)u * kThreads;
+        if (e < e1) P0[e] = zv[u] + beta * pv[u];
+      }
+    }
+  }
+}
+
 // Step B: X += alpha P, R -= alpha AP, Z = M R (CG) or Z = M R (reliable); per column r.r, r.z;
 // per-column convergence, beta, problem bookkeeping.
 template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
   __shared__ double sm[2][kThreads];
-  __shared__ int flag_reliable;
+  __shared__ int flag_any, flag_all;
   const int c = threadIdx.x % K;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
@@ -350,23 +434,45 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
     const double alpha = A.cs[(int64_t)p * K + c].alpha;
-    const double* pc = P.psel ? A.P1 : A.P0;
+    const double* __restrict__ pc = A.P0;
+    double* __restrict__ X = A.X;
+    double* __restrict__ R = A.R;
+    double* __restrict__ Z = A.Z;
+    const double* __restrict__ AP = A.AP;
     const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
     double rr = 0.0, rz = 0.0;
-    for (int64_t idx = (int64_t)r0 * K + threadIdx.x; idx < (int64_t)r1 * K; idx += kThreads) {
-      const int i = (int)(idx / K);
-      double ri;
-      if (reliable) {
-        ri = A.R[idx];
-      } else {
-        A.X[idx] += alpha * pc[idx];
-        ri = A.R[idx] - alpha * A.AP[idx];
-        A.R[idx] = ri;
+    // 4 elements of this thread's column per trip (kThreads is a multiple of K), every load of
+    // the trip issued before any store
+    const int64_t e0 = (int64_t)r0 * K + threadIdx.x, e1 = (int64_t)r1 * K;
+    for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
+      double xv[4], pv[4], rv[4], av[4], dv[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = idx + (int64_t)u * kThreads;
+        const bool ok = e < e1;
+        rv[u] = ok ? R[e] : 0.0;
+        dv[u] = ok ? __ldg(A.dinv + e / K) : 0.0;
+        if (!reliable) {
+          xv[u] = ok ? X[e] : 0.0;
+          pv[u] = ok ? pc[e] : 0.0;
+          av[u] = ok ? AP[e] : 0.0;
+        }
       }
-      const double zi = A.dinv[i] * ri;
-      A.Z[idx] = zi;
-      rr += ri * ri;
-      rz += ri * zi;
+#pragma unroll
+      for (int u = 0; u < 4; ++u) {
+        const int64_t e = idx + (int64_t)u * kThreads;
+        if (e >= e1) break;
+        double ri = rv[u];
+        if (!reliable) {
+          X[e] = xv[u] + alpha * pv[u];
+          ri = rv[u] - alpha * av[u];
+          R[e] = ri;
+        }
+        const double zi = dv[u] * ri;
+        Z[e] = zi;
+        rr += ri * ri;
+        rz += ri * zi;
+      }
     }
     block_col_sums<K>(rr, sm[0]);
     block_col_sums<K>(rz, sm[1]);
@@ -376,7 +482,13 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
     }
     const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
     if (last_of_problem(&A.ps[p].ticket_b, n_it)) {
-      if (threadIdx.x == 0) flag_reliable = 0;
+      // mixed: a column is ready for an FP64 residual replacement once its recursive residual
+      // dropped by delta since the last one or reached tol; the problem replaces when a column
+      // is ready and kMinReliableGap steps have passed, or when every unconverged column is ready
+      if (threadIdx.x == 0) {
+        flag_any = 0;
+        flag_all = 1;
+      }
       __syncthreads();
       if (threadIdx.x < K) {
         double s0 = 0.0, s1 = 0.0;
@@ -395,7 +507,9 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
             if (conv) C.converged = 1;
             if (reliable) C.rmax = sqrt(rrv);
           } else if (conv || sqrt(rrv) < A.delta * C.rmax) {
-            atomicOr(&flag_reliable, 1);
+            atomicOr(&flag_any, 1);
+          } else {
+            atomicAnd(&flag_all, 0);
           }
           if (reliable) {
             C.beta = s1 / C.rz_prev;  // r replaced the recurrence residual of the previous step
@@ -415,7 +529,9 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
         else Pm.reliable += 1;
         int all = 1;
         for (int q = 0; q < K; ++q) all &= A.cs[(int64_t)p * K + q].converged;
-        if (MIXED && !reliable && flag_reliable) {
+        const bool replace = flag_any && (flag_all || Pm.iters - Pm.last_reliable >= kMinReliableGap);
+        if (MIXED && !reliable && replace) {
+          Pm.last_reliable = Pm.iters;
           // FP64 residual replacement next; the search directions wait for it.  rz_old of the
           // columns was advanced above; it is recomputed from the replaced residual.
           Pm.mode = kModeReliable;
@@ -442,7 +558,7 @@ size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct BLayout {
   size_t total;
-  size_t o_R, o_Z, o_P0, o_P1, o_AP, o_part, o_ps, o_cs, o_rem;
+  size_t o_R, o_Z, o_P0, o_AP, o_part, o_ps, o_cs, o_rem;
 };
 
 BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
@@ -457,7 +573,6 @@ BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
   L.o_R = take(panel);
   L.o_Z = take(panel);
   L.o_P0 = take(panel);
-  L.o_P1 = take(panel);
   L.o_AP = take(panel);
   L.o_part = take(sizeof(double) * 2 * (size_t)k * (size_t)n_items);
   L.o_ps = take(sizeof(ProbState) * (size_t)n_problems);
@@ -495,9 +610,11 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
     if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
     for (int q = 0; q < chunk; ++q) {
       if (prec == FEAB_PREC_MIXED) {
+        k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
         k_bstep_a<K, true><<<grid, kThreads, 0, cs>>>(A);
         k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
       } else {
+        k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
         k_bstep_a<K, false><<<grid, kThreads, 0, cs>>>(A);
         k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
       }
@@ -512,14 +629,14 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
     if (fail(cudaGraphLaunch(exec, s))) break;
     if (fail(cudaEventRecord(ev[0], s))) break;
     launched = 1;
-    count_launches(2 * (uint64_t)chunk);
+    count_launches(3 * (uint64_t)chunk);
     while (true) {
       const bool more = launched < max_launch;
       if (more) {
         if (fail(cudaGraphLaunch(exec, s))) break;
         if (fail(cudaEventRecord(ev[launched & 1], s))) break;
         ++launched;
-        count_launches(2 * (uint64_t)chunk);
+        count_launches(3 * (uint64_t)chunk);
       }
       if (fail(cudaEventSynchronize(ev[more ? ((launched - 2) & 1) : ((launched - 1) & 1)]))) break;
       if (((volatile int32_t*)hflag)[0] <= 0 || !more) break;
@@ -582,6 +699,7 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   const int prec = prm->precision;
   if (prec != FEAB_PREC_FP64 && prec != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
   if (prec == FEAB_PREC_MIXED && !D) return FEAB_BAD_ARG;
+  if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return FEAB_BAD_ARG;  // 16-byte panel gathers
   const BLayout L = blayout(M->n, k, bt->n_problems, bt->n_items);
   if (L.total > workspace_bytes) return FEAB_BAD_ARG;
   char* w = static_cast<char*>(workspace);
@@ -615,7 +733,6 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   A.R = reinterpret_cast<double*>(w + L.o_R);
   A.Z = reinterpret_cast<double*>(w + L.o_Z);
   A.P0 = reinterpret_cast<double*>(w + L.o_P0);
-  A.P1 = reinterpret_cast<double*>(w + L.o_P1);
   A.AP = reinterpret_cast<double*>(w + L.o_AP);
   A.part = reinterpret_cast<double*>(w + L.o_part);
   A.ps = reinterpret_cast<ProbState*>(w + L.o_ps);

@@ -398,6 +398,98 @@ __global__ void k_symeig_jacobi(double* A, int k, double* w, double* V, int max_
   }
 }
 
+// FP64 Gram on the CUDA cores: G = X^T X accumulated in FP64 for X (n x 64, FP32 or FP64, row
+// major).  The split-bf16 tensor-core Gram accumulates in FP32, which resolves eigenvalues down to
+// about 1e-6 of the largest; snapshot sets of elastic solutions decay much faster (lambda_10 /
+// lambda_1 ~ 1e-8), and their trailing singular values need FP64 accumulation.
+// One CTA per SM; 256 threads = 4 row groups x 64 threads; thread (bi, bj) of a row group owns
+// G[bi + 8u][bj + 8v] (u, v < 8, interleaved so that shared-memory reads are contiguous across
+// the warp) and accumulates the rows r = rg (mod 4) of each 64-row tile.  The next tile is read
+// into registers while the current one is consumed.  Row groups are summed in a fixed order
+// through shared memory, CTAs by k_gram_reduce64, so G is deterministic.
+constexpr int kGTile = 64;
+constexpr int kGThreads = 256;
+
+template <typename T>
+__device__ __forceinline__ void gram_load_tile(const T* __restrict__ X, int64_t n, int64_t r0, double (&reg)[16]) {
+  // 64 rows x 64 values: thread t loads values t, t + 256, ... (16 per thread), coalesced
+#pragma unroll
+  for (int i = 0; i < 16; ++i) {
+    const int e = threadIdx.x + kGThreads * i;
+    const int r = e >> 6, c = e & 63;
+    reg[i] = (r0 + r < n) ? (double)__ldcs(X + (r0 + r) * kCols + c) : 0.0;
+  }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(kGThreads, 1) k_gram_fp64(const T* __restrict__ X, int64_t n,
+                                                          double* __restrict__ part) {
+  __shared__ double xs[kGTile * kCols];  // 32 KB: one tile, then the row-group reduction
+  const int tid = threadIdx.x, rg = tid >> 6, t = tid & 63, bi = t >> 3, bj = t & 7;
+  double acc[8][8];
+#pragma unroll
+  for (int u = 0; u < 8; ++u)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) acc[u][v] = 0.0;
+  const int64_t tiles = (n + kGTile - 1) / kGTile;
+  double reg[16];
+  int64_t tile = blockIdx.x;
+  if (tile < tiles) gram_load_tile(X, n, tile * kGTile, reg);
+  for (; tile < tiles; tile += gridDim.x) {
+    __syncthreads();  // the previous tile is consumed
+#pragma unroll
+    for (int i = 0; i < 16; ++i) xs[threadIdx.x + kGThreads * i] = reg[i];
+    __syncthreads();
+    if (tile + gridDim.x < tiles) gram_load_tile(X, n, (tile + gridDim.x) * kGTile, reg);
+    for (int r = rg; r < kGTile; r += 4) {  // rows past n were stored as zeros
+      const double* row = xs + r * kCols;
+      double a[8], b[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        a[u] = row[bi + 8 * u];
+        b[u] = row[bj + 8 * u];
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) acc[u][v] = fma(a[u], b[v], acc[u][v]);
+    }
+  }
+  // row groups 0..3 summed in order
+  for (int g = 0; g < 4; ++g) {
+    __syncthreads();
+    if (rg == g) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u)
+#pragma unroll
+        for (int v = 0; v < 8; ++v) {
+          const int idx = (bi + 8 * u) * kCols + bj + 8 * v;
+          xs[idx] = g == 0 ? acc[u][v] : xs[idx] + acc[u][v];
+        }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kCols * kCols; e += kGThreads) part[(int64_t)blockIdx.x * kCols * kCols + e] = xs[e];
+}
+
+// G = sum over CTAs (fixed order) of part[cta], symmetrised.
+__global__ void k_gram_reduce64(const double* __restrict__ part, int ctas, double* __restrict__ G) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= kCols * kCols) return;
+  const int m = idx / kCols, nn = idx % kCols;
+  double s = 0.0, t = 0.0;
+  for (int c = 0; c < ctas; ++c) {
+    s += part[(int64_t)c * kCols * kCols + m * kCols + nn];
+    t += part[(int64_t)c * kCols * kCols + nn * kCols + m];
+  }
+  G[idx] = 0.5 * (s + t);
+}
+
+int gram_fp64_grid(int64_t n) {
+  const int64_t tiles = (n + kGTile - 1) / kGTile;
+  return (int)std::max<int64_t>(1, std::min<int64_t>(tiles, (int64_t)sm_count()));
+}
+
 int gram_grid(int64_t n) {
   const int64_t chunks = (n + kChunk - 1) / kChunk;
   return (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count() * 2));
@@ -424,6 +516,20 @@ extern "C" int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double
   double* part = static_cast<double*>(workspace);
   k_gram_bf16x3<<<grid, kThreadsG, smem, s>>>(X, n, part, error_flag);
   k_gram_reduce<<<(kCols * kCols + 255) / 256, 256, 0, s>>>(part, grid, G);
+  count_launches(2);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
+}
+
+extern "C" int32_t feab_gram_fp64(const void* X, int32_t x_bytes, int64_t n, int32_t k, double* G, void* workspace,
+                                  size_t workspace_bytes, cudaStream_t s) {
+  if (!X || !G || !workspace || n <= 0 || k != kCols || (x_bytes != 4 && x_bytes != 8)) return FEAB_BAD_ARG;
+  if (feab_gram_workspace_bytes(n, k) > workspace_bytes) return FEAB_BAD_ARG;
+  const int grid = gram_fp64_grid(n);
+  double* part = static_cast<double*>(workspace);
+  if (x_bytes == 4) k_gram_fp64<float><<<grid, kGThreads, 0, s>>>(static_cast<const float*>(X), n, part);
+  else k_gram_fp64<double><<<grid, kGThreads, 0, s>>>(static_cast<const double*>(X), n, part);
+  k_gram_reduce64<<<(kCols * kCols + 255) / 256, 256, 0, s>>>(part, grid, G);
   count_launches(2);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;

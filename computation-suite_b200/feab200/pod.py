@@ -2,10 +2,16 @@
 
 ``PodBasis.fit`` keeps the reference's signature and rank rule (n_modes / energy_threshold,
 _select_rank pod.py:163-176).  The FP64 economy SVD of the reference (pod.py:140-147) is
-replaced by the method of snapshots: the 64 x 64 Gram matrix X^T X on the tensor cores
-(split-bf16 x3 products, FP32 accumulate, FP64 across chunks; feab_gram_bf16x3), its FP64
-eigenvalues by a one-CTA Jacobi solver (feab_symeig_jacobi), singular values sqrt(lambda),
-and modes U = X V / sigma.
+replaced by the method of snapshots: the 64 x 64 Gram matrix X^T X, its FP64 eigenvalues by a
+one-CTA Jacobi solver (feab_symeig_jacobi), singular values sqrt(lambda), and modes
+U = X V / sigma.  Two Gram kernels:
+
+* ``gram="fp64"`` (default): FP64 accumulation on the CUDA cores (feab_gram_fp64), which keeps
+  trailing singular values of fast-decaying snapshot spectra (sigma_10 / sigma_1 ~ 1e-4 for
+  elastic solutions) to FP32-input accuracy;
+* ``gram="bf16x3"``: the tensor cores (split-bf16 x3 products, FP32 accumulate, FP64 across
+  chunks; feab_gram_bf16x3) -- resolves eigenvalues down to ~1e-6 of the largest, i.e. the
+  leading singular values only.
 """
 from __future__ import annotations
 
@@ -36,6 +42,23 @@ def gram_bf16x3(X):
     L.raise_for(rc, "gram_bf16x3")
     if int(err.item()):
         raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
+    return G
+
+
+def gram_fp64(X):
+    """G = X^T X (FP64, 64 x 64) accumulated in FP64 for a device panel X (n x 64, FP32 or
+    FP64, row major)."""
+    X = X.contiguous()
+    if X.dtype not in (torch.float32, torch.float64) or X.ndim != 2 or X.shape[1] != MAX_SNAPSHOTS:
+        raise ValueError("gram_fp64 needs an (n, 64) float32 or float64 device panel")
+    dev = X.device
+    n = X.shape[0]
+    wbytes = int(L.lib.feab_gram_workspace_bytes(n, MAX_SNAPSHOTS))
+    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    G = torch.empty((MAX_SNAPSHOTS, MAX_SNAPSHOTS), dtype=torch.float64, device=dev)
+    rc = L.lib.feab_gram_fp64(L.dptr(X), X.element_size(), n, MAX_SNAPSHOTS, L.dptr(G), L.dptr(ws), wbytes,
+                              L.stream_ptr(dev))
+    L.raise_for(rc, "gram_fp64")
     return G
 
 
@@ -75,7 +98,7 @@ class PodBasis:
         self.mass_weighted = False
         self.M = None
 
-    def fit(self, snapshots, n_modes=None, energy_threshold=None, M=None, device=None):
+    def fit(self, snapshots, n_modes=None, energy_threshold=None, M=None, device=None, gram="fp64"):
         if n_modes is None and energy_threshold is None:
             raise ValueError("fit() needs at least one of n_modes, energy_threshold")
         if M is not None:
@@ -87,9 +110,12 @@ class PodBasis:
         n, k = X.shape
         if k > MAX_SNAPSHOTS:
             raise NotImplementedError(f"PodBasis.fit: at most {MAX_SNAPSHOTS} snapshots per panel on the GPU path")
-        X32 = torch.zeros((n, MAX_SNAPSHOTS), dtype=torch.float32, device=dev)
-        X32[:, :k] = X.to(torch.float32)
-        G = gram_bf16x3(X32)
+        if gram not in ("fp64", "bf16x3"):
+            raise ValueError("gram must be 'fp64' or 'bf16x3'")
+        dt = torch.float32 if gram == "bf16x3" else torch.float64
+        Xp = torch.zeros((n, MAX_SNAPSHOTS), dtype=dt, device=dev)
+        Xp[:, :k] = X.to(dt)
+        G = gram_bf16x3(Xp) if gram == "bf16x3" else gram_fp64(Xp)
         w, V = symeig(G)
         S = torch.sqrt(torch.clamp(w[: min(k, n)], min=0.0))
         S_host = S.cpu().numpy()

@@ -282,8 +282,8 @@ int32_t feab_csr_spmv(const feab_csr* A, const feab_sell_operator* sell, int32_t
  * runs its own CG recurrence (preconditioned_cg, iterative_solvers.py:434-481) -- the
  * iterative counterpart of solve_batched / solve_static_batched (batched_solve.py:44-164),
  * which factorise once for many columns.  precision: FEAB_PREC_FP64 or FEAB_PREC_MIXED
- * (diff != NULL).  Synchronous; per-column iterations / FP64 relative residuals and
- * per-problem status go to the optional host arrays. */
+ * (diff != NULL).  X must be 16-byte aligned.  Synchronous; per-column iterations / FP64
+ * relative residuals and per-problem status go to the optional host arrays. */
 typedef struct feab_batch {
   int32_t n_problems;
   int32_t k;                       /* panel width                                   */
@@ -314,6 +314,14 @@ size_t feab_gram_workspace_bytes(int64_t n, int32_t k);
 
 int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double* G, void* workspace, size_t workspace_bytes,
                          int32_t* error_flag, cudaStream_t stream);
+
+/* G = X^T X (64 x 64, FP64) accumulated in FP64 on the CUDA cores, for X (n x 64, row major)
+ * of FP32 (x_bytes = 4) or FP64 (x_bytes = 8) values; the same workspace as feab_gram_bf16x3.
+ * The accurate Gram for snapshot sets whose spectrum decays faster than FP32 accumulation
+ * resolves (the FP64 SVD of PodBasis._fit_standard, rom_engine/src/rom_engine/pod.py:140-147,
+ * gets such trailing singular values right).  Asynchronous on the stream; deterministic. */
+int32_t feab_gram_fp64(const void* X, int32_t x_bytes, int64_t n, int32_t k, double* G, void* workspace,
+                       size_t workspace_bytes, cudaStream_t stream);
 
 /* Cyclic Jacobi eigensolver (one CTA, FP64) for a symmetric k x k matrix (k <= 64) in device
  * memory: eigenvalues descending into evals, eigenvectors (columns) into evecs (may be NULL).

@@ -1,5 +1,6 @@
-"""POD on the tensor cores: Gram X^T X (split-bf16 x3) + FP64 Jacobi eigensolve, against the
-reference's SVD singular values (tests/golden/pod_small.npz) and the FP64 oracle."""
+"""POD: Gram X^T X (FP64 on the CUDA cores, or split-bf16 x3 on the tensor cores) + FP64 Jacobi
+eigensolve, against the reference's SVD singular values (tests/golden/pod_small.npz) and the
+FP64 oracle."""
 import numpy as np
 import pytest
 import torch
@@ -27,6 +28,23 @@ def test_gram_is_deterministic():
     assert torch.equal(gram_bf16x3(X), gram_bf16x3(X))
 
 
+@pytest.mark.parametrize("dtype", [np.float32, np.float64])
+def test_gram_fp64_matches_numpy(dtype):
+    from feab200.pod import gram_fp64
+    rng = np.random.default_rng(2)
+    n = 64 * 301 + 37                     # many tiles, more tiles than CTAs, a ragged last tile
+    X = (rng.standard_normal((n, 64)) * np.logspace(0, -6, 64)[None, :]).astype(dtype)
+    G = gram_fp64(torch.as_tensor(X).cuda()).cpu().numpy()
+    ref = X.astype(np.float64).T @ X.astype(np.float64)
+    # FP64 accumulation: entrywise relative to sqrt(G_ii G_jj), far below FP32 resolution
+    scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref)))
+    assert np.abs(G - ref).max() / 1.0 <= 1e-12 * scale.max()
+    assert (np.abs(G - ref) / scale).max() < 1e-13
+    assert np.array_equal(G, G.T)
+    Xt = torch.as_tensor(X).cuda()
+    assert torch.equal(gram_fp64(Xt), gram_fp64(Xt))   # deterministic
+
+
 def test_symeig_jacobi():
     from feab200.pod import symeig
     rng = np.random.default_rng(1)
@@ -44,10 +62,17 @@ def test_pod_singular_values_match_reference(golden):
     g = golden("pod_small")
     basis = PodBasis().fit(g["X"], n_modes=10)
     s, ref = basis.singular_values, g["singular_values"]
-    # leading values to bf16x3 accuracy; the reference's spectrum decays by 1e-11 overall
-    assert np.abs(s[0] - ref[0]) / ref[0] < 1e-4
-    assert np.all(np.abs(s[:3] - ref[:3]) / ref[:3] < 1e-2)
+    # the reference's spectrum spans 12 decades; a Gram (eigenvalues = sigma^2) resolves
+    # sigma_k to ~1e-16 (sigma_1 / sigma_k)^2 in FP64: the first six to 1e-6, the first eight
+    # to 1e-2
+    rel = np.abs(s - ref[: len(s)]) / ref[: len(s)]
+    assert np.all(rel[:6] < 1e-6), rel
+    assert np.all(rel[:8] < 1e-2), rel
     assert basis.n_modes == 10
+    # the tensor-core Gram: leading values to its FP32-accumulation accuracy
+    s16 = PodBasis().fit(g["X"], n_modes=10, gram="bf16x3").singular_values
+    assert np.abs(s16[0] - ref[0]) / ref[0] < 1e-4
+    assert np.all(np.abs(s16[:3] - ref[:3]) / ref[:3] < 1e-2)
 
 
 def test_pod_on_solution_snapshots():
@@ -60,4 +85,7 @@ def test_pod_on_solution_snapshots():
     s = PodBasis().fit(X, n_modes=10).singular_values
     ref = O.pod_singular_values(X)
     rel = np.abs(s[:10] - ref[:10]) / ref[:10]
-    assert rel[0] < 1e-5 and np.all(rel[:5] < 1e-3), rel
+    assert np.all(rel[:10] < 1e-8), rel
+    s16 = PodBasis().fit(X, n_modes=10, gram="bf16x3").singular_values
+    rel16 = np.abs(s16[:10] - ref[:10]) / ref[:10]
+    assert rel16[0] < 1e-5 and np.all(rel16[:5] < 1e-3), rel16

@@ -105,7 +105,15 @@ __device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
 // form for the difference operator), filled with coalesced loads before the SpMM reads them as
 // broadcasts; groups longer than kStageCols are staged in pieces.
 constexpr int kStageCols = 128;
-constexpr int kUnroll = 4;  // matrix columns whose panel rows a lane gathers before using any
+// matrix columns whose panel rows a lane gathers before using any
+#ifndef FEAB_BLOCK_UNROLL
+#define FEAB_BLOCK_UNROLL 8
+#endif
+constexpr int kUnroll = FEAB_BLOCK_UNROLL;
+// minimum resident CTAs per SM of the SpMM kernel (register budget)
+#ifndef FEAB_BLOCK_MINB
+#define FEAB_BLOCK_MINB 1
+#endif
 
 struct GroupStage {
   int col[kStageCols];
@@ -200,11 +208,11 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
         const int m = m0 + u * MPW;
         if (m >= nc) break;
         const double w0 = st.val[0][m], w1 = st.val[1][m], w2 = st.val[2][m];
-        const unsigned jc = t[u] >> 30;
 #pragma unroll
         for (int q = 0; q < CPL; ++q) {
-          // difference form: padding columns carry value 0 and point at the own node (d = 0)
-          const double d = DIFF ? xv[u][q] - (jc == 0u ? xs[0][q] : (jc == 1u ? xs[1][q] : xs[2][q])) : xv[u][q];
+          // difference form as sum w x_b + T x_a (T folded into S at build time); padding
+          // columns carry value 0
+          const double d = xv[u][q];
           acc[0][q] = fma(w0, d, acc[0][q]);
           acc[1][q] = fma(w1, d, acc[1][q]);
           acc[2][q] = fma(w2, d, acc[2][q]);
@@ -306,7 +314,7 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
 // Step A: AP = K P (P updated by k_bstep_p; or, in a reliable step, R = B - K64 X);
 // per-column partial p.Ap (or r.r).
 template <int K, bool MIXED>
-__global__ void __launch_bounds__(kThreads) k_bstep_a(BArgs A) {
+__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
   __shared__ double sm[kWarps][K];
@@ -426,6 +434,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
 template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
   __shared__ double sm[2][kThreads];
+  __shared__ double smv[2][2 * kThreads];
   __shared__ int flag_any, flag_all;
   const int c = threadIdx.x % K;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
@@ -433,52 +442,117 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
     const ProbState P = A.ps[p];
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
-    const double alpha = A.cs[(int64_t)p * K + c].alpha;
     const double* __restrict__ pc = A.P0;
     double* __restrict__ X = A.X;
     double* __restrict__ R = A.R;
     double* __restrict__ Z = A.Z;
     const double* __restrict__ AP = A.AP;
     const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
-    double rr = 0.0, rz = 0.0;
-    // 4 elements of this thread's column per trip (kThreads is a multiple of K), every load of
-    // the trip issued before any store
-    const int64_t e0 = (int64_t)r0 * K + threadIdx.x, e1 = (int64_t)r1 * K;
-    for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
-      double xv[4], pv[4], rv[4], av[4], dv[4];
+    if constexpr (K >= 2) {
+      // two adjacent columns c2, c2 + 1 per thread with 16-byte accesses, two pairs per trip,
+      // every load of the trip issued before any store
+      const int c2 = 2 * (threadIdx.x % (K / 2));
+      const double al0 = A.cs[(int64_t)p * K + c2].alpha, al1 = A.cs[(int64_t)p * K + c2 + 1].alpha;
+      double rr0 = 0.0, rr1 = 0.0, rz0 = 0.0, rz1 = 0.0;
+      const int64_t q0 = (int64_t)r0 * (K / 2) + threadIdx.x, q1 = (int64_t)r1 * (K / 2);
+      const double2* __restrict__ P2 = reinterpret_cast<const double2*>(pc);
+      const double2* __restrict__ AP2 = reinterpret_cast<const double2*>(AP);
+      double2* __restrict__ X2 = reinterpret_cast<double2*>(X);
+      double2* __restrict__ R2 = reinterpret_cast<double2*>(R);
+      double2* __restrict__ Z2 = reinterpret_cast<double2*>(Z);
+      for (int64_t q = q0; q < q1; q += 2 * kThreads) {
+        double2 xv[2], pv[2], rv[2], av[2];
+        double dv[2];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int64_t e = idx + (int64_t)u * kThreads;
-        const bool ok = e < e1;
-        rv[u] = ok ? R[e] : 0.0;
-        dv[u] = ok ? __ldg(A.dinv + e / K) : 0.0;
-        if (!reliable) {
-          xv[u] = ok ? X[e] : 0.0;
-          pv[u] = ok ? pc[e] : 0.0;
-          av[u] = ok ? AP[e] : 0.0;
+        for (int u = 0; u < 2; ++u) {
+          const int64_t e = q + (int64_t)u * kThreads;
+          const bool ok = e < q1;
+          rv[u] = ok ? R2[e] : make_double2(0.0, 0.0);
+          dv[u] = ok ? __ldg(A.dinv + e / (K / 2)) : 0.0;
+          if (!reliable) {
+            xv[u] = ok ? X2[e] : make_double2(0.0, 0.0);
+            pv[u] = ok ? P2[e] : make_double2(0.0, 0.0);
+            av[u] = ok ? AP2[e] : make_double2(0.0, 0.0);
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int64_t e = q + (int64_t)u * kThreads;
+          if (e >= q1) break;
+          double ri0 = rv[u].x, ri1 = rv[u].y;
+          if (!reliable) {
+            X2[e] = make_double2(xv[u].x + al0 * pv[u].x, xv[u].y + al1 * pv[u].y);
+            ri0 = rv[u].x - al0 * av[u].x;
+            ri1 = rv[u].y - al1 * av[u].y;
+            R2[e] = make_double2(ri0, ri1);
+          }
+          const double zi0 = dv[u] * ri0, zi1 = dv[u] * ri1;
+          Z2[e] = make_double2(zi0, zi1);
+          rr0 += ri0 * ri0;
+          rr1 += ri1 * ri1;
+          rz0 += ri0 * zi0;
+          rz1 += ri1 * zi1;
         }
       }
-#pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int64_t e = idx + (int64_t)u * kThreads;
-        if (e >= e1) break;
-        double ri = rv[u];
-        if (!reliable) {
-          X[e] = xv[u] + alpha * pv[u];
-          ri = rv[u] - alpha * av[u];
-          R[e] = ri;
+      // per-column sums: entry 2t + h holds column (2t + h) % K; fold entries s apart (s >= K)
+      smv[0][2 * threadIdx.x] = rr0;
+      smv[0][2 * threadIdx.x + 1] = rr1;
+      smv[1][2 * threadIdx.x] = rz0;
+      smv[1][2 * threadIdx.x + 1] = rz1;
+      for (int sh = kThreads; sh >= K; sh >>= 1) {
+        __syncthreads();
+        if (threadIdx.x < sh) {
+          smv[0][threadIdx.x] += smv[0][threadIdx.x + sh];
+          smv[1][threadIdx.x] += smv[1][threadIdx.x + sh];
         }
-        const double zi = dv[u] * ri;
-        Z[e] = zi;
-        rr += ri * ri;
-        rz += ri * zi;
       }
-    }
-    block_col_sums<K>(rr, sm[0]);
-    block_col_sums<K>(rz, sm[1]);
-    if (threadIdx.x < K) {
-      A.part[(int64_t)it * 2 * K + c] = sm[0][c];
-      A.part[(int64_t)it * 2 * K + K + c] = sm[1][c];
+      __syncthreads();
+      if (threadIdx.x < K) {
+        A.part[(int64_t)it * 2 * K + c] = smv[0][c];
+        A.part[(int64_t)it * 2 * K + K + c] = smv[1][c];
+      }
+    } else {
+      const double alpha = A.cs[(int64_t)p * K + c].alpha;
+      double rr = 0.0, rz = 0.0;
+      // 4 elements of this thread's column per trip (kThreads is a multiple of K), every load of
+      // the trip issued before any store
+      const int64_t e0 = (int64_t)r0 * K + threadIdx.x, e1 = (int64_t)r1 * K;
+      for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
+        double xv[4], pv[4], rv[4], av[4], dv[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = idx + (int64_t)u * kThreads;
+          const bool ok = e < e1;
+          rv[u] = ok ? R[e] : 0.0;
+          dv[u] = ok ? __ldg(A.dinv + e / K) : 0.0;
+          if (!reliable) {
+            xv[u] = ok ? X[e] : 0.0;
+            pv[u] = ok ? pc[e] : 0.0;
+            av[u] = ok ? AP[e] : 0.0;
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = idx + (int64_t)u * kThreads;
+          if (e >= e1) break;
+          double ri = rv[u];
+          if (!reliable) {
+            X[e] = xv[u] + alpha * pv[u];
+            ri = rv[u] - alpha * av[u];
+            R[e] = ri;
+          }
+          const double zi = dv[u] * ri;
+          Z[e] = zi;
+          rr += ri * ri;
+          rz += ri * zi;
+        }
+      }
+      block_col_sums<K>(rr, sm[0]);
+      block_col_sums<K>(rz, sm[1]);
+      if (threadIdx.x < K) {
+        A.part[(int64_t)it * 2 * K + c] = sm[0][c];
+        A.part[(int64_t)it * 2 * K + K + c] = sm[1][c];
+      }
     }
     const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
     if (last_of_problem(&A.ps[p].ticket_b, n_it)) {

@@ -658,7 +658,7 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
   }
   for (int k = 0; k < f; ++k) {
     const int s0 = row_ptr[r0 + k];
-    double sj[3] = {0.0, 0.0, 0.0};
+    double sj[3] = {0.0, 0.0, 0.0}, tj[3] = {0.0, 0.0, 0.0};
     for (int cb = 0; cb < len; cb += 32) {
       const int c = cb + lane;
       double v = 0.0;
@@ -675,10 +675,20 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
           vlo[v0 + k * lp + p] = (uint16_t)((bits >> 16) & 0xffffull);
         }
       }
+      // rounded value of an off-node column (0 for own columns and past the end)
+      double wv = 0.0;
+      if (c < len && (c < own || c >= own + f)) {
+        const unsigned long long bw = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
+        wv = __longlong_as_double((long long)(bw & ~0xffffull));
+      }
       for (int u = 0; u < 32; ++u) {
         const double vu = __shfl_sync(FEAB_FULL_MASK, v, u);
+        const double wu = __shfl_sync(FEAB_FULL_MASK, wv, u);
         const int ju = __shfl_sync(FEAB_FULL_MASK, j, u);
-        if (cb + u < len) sj[ju] += vu;
+        if (cb + u < len) {
+          sj[ju] += vu;
+          tj[ju] += wu;
+        }
       }
     }
     // padding: own first free DOF, value 0
@@ -687,7 +697,13 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
       vhi[v0 + k * lp + p] = 0u;
       vlo[v0 + k * lp + p] = 0;
     }
-    if (lane < 3) Ssum[(int64_t)(r0 + k) * 3 + lane] = lane == 0 ? sj[0] : (lane == 1 ? sj[1] : sj[2]);
+    // T = S - W (S: all exact values of component j, W: the rounded off-node ones), so that
+    // sum_{b != a} w (x_b - x_a) + S x_a = sum_{b != a} w x_b + T x_a exactly
+    if (lane < 3) {
+      const double sv = lane == 0 ? sj[0] : (lane == 1 ? sj[1] : sj[2]);
+      const double tv = lane == 0 ? tj[0] : (lane == 1 ? tj[1] : tj[2]);
+      Ssum[(int64_t)(r0 + k) * 3 + lane] = sv - tv;
+    }
   }
 }
 

@@ -83,8 +83,7 @@ __global__ void k_sell_widths(int32_t n_groups, int32_t n_slices, int kind, int3
 }
 
 // Pass 2, one warp per slice, lane l writing group 32 s + l: columns, values (FP64 or rounded to
-// 36 mantissa bits), and for the difference form the free-DOF mask and the row-block sums
-// S[r][j] = sum over row r's columns of DOF component j, summed by the lane in column order.
+// 36 mantissa bits), and for the mixed kind the free-DOF mask and the own-node terms T (below).
 __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_t n_slices, int kind,
                                                         const int32_t* __restrict__ group_ptr,
                                                         const int32_t* __restrict__ row_ptr,
@@ -154,11 +153,24 @@ __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_
     }
   }
   if (diff && valid) {
+    // T[r][j] = S[r][j] - W[r][j]: S sums all of row r's exact values of DOF component j, W its
+    // rounded off-node values of component j (both in column order).  Then
+    //   sum_{b != a} w (x_b - x_a) + S x_a  =  sum_{b != a} w x_b + T x_a
+    // exactly, so the kernel applies the plain form to the rounded values plus T on the own node,
+    // with the same value-rounding error as the difference form.
     for (int k = 0; k < f; ++k) {
       const int sk = row_ptr[r0 + k];
-      double sj[3] = {0.0, 0.0, 0.0};
-      for (int c = 0; c < len; ++c) sj[dof_of[col_idx[sk + c]] % 3] += vals[sk + c];
-      for (int j = 0; j < 3; ++j) Ssum[(int64_t)(r0 + k) * 3 + j] = sj[j];
+      double sj[3] = {0.0, 0.0, 0.0}, wj[3] = {0.0, 0.0, 0.0};
+      for (int c = 0; c < len; ++c) {
+        const int jc = dof_of[col_idx[sk + c]] % 3;
+        const double v = vals[sk + c];
+        sj[jc] += v;
+        if (c < own || c >= own + f) {
+          const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
+          wj[jc] += __longlong_as_double((long long)(bits & ~0xffffull));
+        }
+      }
+      for (int j = 0; j < 3; ++j) Ssum[(int64_t)(r0 + k) * 3 + j] = sj[j] - wj[j];
     }
   }
 }

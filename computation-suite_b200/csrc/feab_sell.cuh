@@ -81,8 +81,10 @@ __device__ __forceinline__ double sell_dec48(uint32_t hi, uint16_t lo) {
   return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
 }
 
-// acc[k] = (K x)[r0 + k] for the lane's group, x read through xf(column).  For the difference
-// form xs[j] = x of the node's own DOF component j (0 when that component is fixed).
+// acc[k] = (K x)[r0 + k] for the lane's group, x read through xf(column).  Mixed kind: the
+// difference form sum_{b != a} w (x_b - x_a) + S x_a, evaluated as sum_{b != a} w x_b + T x_a
+// with T = S - sum_{b != a} w precomputed (the same value exactly, so the same rounding error of
+// the 36-bit values); xs[j] = x of the node's own DOF component j (0 when that component is fixed).
 template <int KIND, typename XF>
 __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lane, const SellLane& L, XF xf,
                                            double (&acc)[3], double (&xs)[3]) {
@@ -158,10 +160,7 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
       } else {
         double d[4];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const unsigned jc = t[nb][u] >> 30;
-          d[u] = xf((int)(t[nb][u] & 0x3fffffffu)) - (jc == 0u ? xs[0] : (jc == 1u ? xs[1] : xs[2]));
-        }
+        for (int u = 0; u < 4; ++u) d[u] = xf((int)(t[nb][u] & 0x3fffffffu));
         const uint4* hh = h[nb];
         const uint2* ll = l[nb];
         a0 = fma(sell_dec48(hh[0].x, (uint16_t)(ll[0].x & 0xffffu)), d[0], a0);

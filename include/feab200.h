@@ -71,7 +71,9 @@ typedef struct feab_csr {
 
 /* Difference-form operator built from the FP64 CSR by feab_diff_operator_build (storage is
  * caller memory, feab_diff_operator_bytes).  Applies y_a = sum_{b!=a} K_ab (x_b - x_a) + S_a x_a
- * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64.
+ * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64,
+ * evaluated as sum_{b!=a} K_ab x_b + T_a x_a with T_a = S_a - W_a, W_a = sum_{b!=a} K_ab over the
+ * rounded values: the same value, so the same rounding error; S holds T.
  * Layout per node row group g (the f rows of one node): its off-node columns, padded to a
  * multiple of 4 (Lp_g), start at goff[g] in tcol; its values start at voff[g], row-major
  * (f rows x Lp_g), so every 4-column quad is one 16-byte (vhi) + 8-byte (vlo) load.  Padding
@@ -81,7 +83,7 @@ typedef struct feab_diff_operator {
   uint32_t* vhi;     /* sum f_g Lp_g: upper 32 bits of the rounded double   */
   uint16_t* vlo;     /* sum f_g Lp_g: next 16 bits                          */
   uint8_t* gmask;    /* n_groups: free-DOF mask of the group's node         */
-  double* S;         /* 3 n: row-block sums per DOF component               */
+  double* S;         /* 3 n: own-node terms T = S - W per DOF component      */
   int32_t* goff;     /* n_groups + 1: first tagged column of each group     */
   int32_t* voff;     /* n_groups + 1: first value of each group             */
 } feab_diff_operator;
@@ -107,7 +109,7 @@ typedef struct feab_sell_operator {
   uint32_t* vhi;     /* MIXED kind: 96 per step                                 */
   uint16_t* vlo;     /* MIXED kind: 96 per step                                 */
   uint8_t* gmask;    /* MIXED kind: n_groups free-DOF masks                     */
-  double* S;         /* MIXED kind: 3 n row-block sums                          */
+  double* S;         /* MIXED kind: 3 n own-node terms T = S - W               */
 } feab_sell_operator;
 
 typedef struct feab_pcg_params {

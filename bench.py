@@ -506,7 +506,9 @@ def workload_snapshot(args):
         res[prec] = (e0.elapsed_time(e1), Xp, rp)
     X = res["mixed"][1]
     X32 = X.to(torch.float32).contiguous()
-    gram_ms, G = _timed(lambda: gram_bf16x3(X32), 5, 2)
+    gram_ms, (G, gflag) = _timed(lambda: gram_bf16x3(X32, check=False), 5, 2)
+    if int(gflag.item()):
+        raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
     gram64_ms, G64 = _timed(lambda: gram_fp64(X32), 5, 2)
     eig_ms, (w, V) = _timed(lambda: symeig(G), 3, 1)
     w64, _ = symeig(G64)
@@ -537,25 +539,36 @@ def workload_snapshot(args):
 
 
 def workload_gram(args):
-    """The tensor-core Gram + FP64 eigensolve alone on a seeded random 1,382,976 x 64 FP32 panel
-    (the snapshot set's size), L2 flushed before each timed launch."""
+    """The tensor-core Gram (and, beside it, the FP64 CUDA-core Gram) alone on a seeded random
+    1,382,976 x 64 FP32 panel (the snapshot set's size), L2 flushed before each timed launch."""
     import torch
-    from feab200.pod import gram_bf16x3, symeig
+    from feab200.pod import gram_bf16x3, gram_fp64, symeig
     n, k = 1_382_976, 64
     g = torch.Generator(device="cuda").manual_seed(5)
     X = torch.randn((n, k), generator=g, device="cuda", dtype=torch.float32)
     flush = L2Flush("cuda")
+    ws = torch.empty(int(__import__("feab200")._lib.lib.feab_gram_workspace_bytes(n, k)), dtype=torch.uint8,
+                     device="cuda")
     for _ in range(args.warmup):
         gram_bf16x3(X)
-    times = []
+    times, times64, flags = [], [], []
     for _ in range(args.steps):
-        flush()
-        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record()
-        G = gram_bf16x3(X)
-        b.record()
-        torch.cuda.synchronize()
-        times.append(a.elapsed_time(b))
+        for fn, out in ((lambda: gram_bf16x3(X, check=False, workspace=ws), times),
+                        (lambda: gram_fp64(X, workspace=ws), times64)):
+            flush()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            r = fn()
+            b.record()
+            torch.cuda.synchronize()
+            out.append(a.elapsed_time(b))
+            if isinstance(r, tuple):
+                G, f = r
+                flags.append(int(f.item()))
+    if any(flags):
+        raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
+    ms64 = statistics.mean(times64)
+    G64 = gram_fp64(X)
     ms = statistics.mean(times)
     ref = X.double().T @ X.double()
     err = float((G - ref).abs().max() / ref.abs().max())
@@ -566,7 +579,10 @@ def workload_gram(args):
             "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3), "bytes_per_launch": nbytes,
                          "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})"},
-            "gram_rel_err_vs_fp64": err, "lambda_max": float(w[0])}
+            "gram_rel_err_vs_fp64": err, "lambda_max": float(w[0]),
+            "gram_fp64_cuda_cores_ms": round(ms64, 4),
+            "gram_fp64_rel_err_vs_fp64": float((G64 - ref).abs().max() / ref.abs().max()),
+            "timing": "CUDA events around the kernel launches only, L2 flushed before each"}
 
 
 def workload_spmv(args):

@@ -110,6 +110,10 @@ constexpr int kStageCols = 128;
 #define FEAB_BLOCK_UNROLL 8
 #endif
 constexpr int kUnroll = FEAB_BLOCK_UNROLL;
+// 1: the vector pass moves two adjacent panel columns per 16-byte access
+#ifndef FEAB_BLOCK_VECB
+#define FEAB_BLOCK_VECB 1
+#endif
 // minimum resident CTAs per SM of the SpMM kernel (register budget)
 #ifndef FEAB_BLOCK_MINB
 #define FEAB_BLOCK_MINB 1
@@ -175,17 +179,35 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
   }
   for (int cb = 0; cb < len; cb += kStageCols) {
     const int nc = min(kStageCols, len - cb);
-    for (int m = lane; m < nc; m += 32) {
-      if (!DIFF) {
+    if (!DIFF) {
+      for (int m = lane; m < nc; m += 32) {
         st.col[m] = __ldg(A.col_idx + s0 + cb + m);
 #pragma unroll
         for (int k = 0; k < 3; ++k) st.val[k][m] = k < f ? __ldg(A.vals64 + s0 + k * len + cb + m) : 0.0;
-      } else {
-        st.col[m] = __ldg(A.tcol + c0 + cb + m);
+      }
+    } else {
+      // the difference-form operator is packed in 4-column quads (group offsets and lengths are
+      // multiples of 4): one 16-byte column load and, per row, a 16 + 8-byte value load per quad
+      for (int mq = lane; mq < (nc >> 2); mq += 32) {
+        const int m = 4 * mq;
+        const uint4 tq = __ldg(reinterpret_cast<const uint4*>(A.tcol + c0 + cb + m));
+        st.col[m] = (int)tq.x;
+        st.col[m + 1] = (int)tq.y;
+        st.col[m + 2] = (int)tq.z;
+        st.col[m + 3] = (int)tq.w;
 #pragma unroll
-        for (int k = 0; k < 3; ++k)
-          st.val[k][m] = k < f ? dec48(__ldg(A.vhi + s0 + k * len + cb + m), __ldg(A.vlo + s0 + k * len + cb + m))
-                               : 0.0;
+        for (int k = 0; k < 3; ++k) {
+          if (k < f) {
+            const uint4 h = __ldg(reinterpret_cast<const uint4*>(A.vhi + s0 + k * len + cb + m));
+            const uint2 l = __ldg(reinterpret_cast<const uint2*>(A.vlo + s0 + k * len + cb + m));
+            st.val[k][m] = dec48(h.x, (uint16_t)(l.x & 0xffffu));
+            st.val[k][m + 1] = dec48(h.y, (uint16_t)(l.x >> 16));
+            st.val[k][m + 2] = dec48(h.z, (uint16_t)(l.y & 0xffffu));
+            st.val[k][m + 3] = dec48(h.w, (uint16_t)(l.y >> 16));
+          } else {
+            st.val[k][m] = st.val[k][m + 1] = st.val[k][m + 2] = st.val[k][m + 3] = 0.0;
+          }
+        }
       }
     }
     __syncwarp();
@@ -448,7 +470,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
     double* __restrict__ Z = A.Z;
     const double* __restrict__ AP = A.AP;
     const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
-    if constexpr (K >= 2) {
+    if constexpr (K >= 2 && FEAB_BLOCK_VECB) {
       // two adjacent columns c2, c2 + 1 per thread with 16-byte accesses, two pairs per trip,
       // every load of the trip issued before any store
       const int c2 = 2 * (threadIdx.x % (K / 2));

@@ -26,35 +26,41 @@ from .device import cuda_device
 MAX_SNAPSHOTS = 64
 
 
-def gram_bf16x3(X):
-    """G = X^T X (FP64, 64 x 64) of a device panel X (n x 64, FP32, row major)."""
+def gram_bf16x3(X, check=True, workspace=None):
+    """G = X^T X (FP64, 64 x 64) of a device panel X (n x 64, FP32, row major).  With
+    check=False the call stays asynchronous and returns (G, error_flag): the device flag is
+    non-zero if a bounded wait timed out, and the caller reads it later."""
     X = X.contiguous()
     if X.dtype != torch.float32 or X.ndim != 2 or X.shape[1] != MAX_SNAPSHOTS:
         raise ValueError("gram_bf16x3 needs an (n, 64) float32 device panel")
     dev = X.device
     n = X.shape[0]
     wbytes = int(L.lib.feab_gram_workspace_bytes(n, MAX_SNAPSHOTS))
-    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    ws = workspace if workspace is not None and workspace.numel() >= wbytes else torch.empty(wbytes, dtype=torch.uint8,
+                                                                                               device=dev)
     G = torch.empty((MAX_SNAPSHOTS, MAX_SNAPSHOTS), dtype=torch.float64, device=dev)
     err = torch.zeros(1, dtype=torch.int32, device=dev)
     rc = L.lib.feab_gram_bf16x3(L.dptr(X), n, MAX_SNAPSHOTS, L.dptr(G), L.dptr(ws), wbytes, L.dptr(err),
                                 L.stream_ptr(dev))
     L.raise_for(rc, "gram_bf16x3")
+    if not check:
+        return G, err
     if int(err.item()):
         raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
     return G
 
 
-def gram_fp64(X):
+def gram_fp64(X, workspace=None):
     """G = X^T X (FP64, 64 x 64) accumulated in FP64 for a device panel X (n x 64, FP32 or
-    FP64, row major)."""
+    FP64, row major).  Asynchronous on the current stream."""
     X = X.contiguous()
     if X.dtype not in (torch.float32, torch.float64) or X.ndim != 2 or X.shape[1] != MAX_SNAPSHOTS:
         raise ValueError("gram_fp64 needs an (n, 64) float32 or float64 device panel")
     dev = X.device
     n = X.shape[0]
     wbytes = int(L.lib.feab_gram_workspace_bytes(n, MAX_SNAPSHOTS))
-    ws = torch.empty(wbytes, dtype=torch.uint8, device=dev)
+    ws = workspace if workspace is not None and workspace.numel() >= wbytes else torch.empty(wbytes, dtype=torch.uint8,
+                                                                                               device=dev)
     G = torch.empty((MAX_SNAPSHOTS, MAX_SNAPSHOTS), dtype=torch.float64, device=dev)
     rc = L.lib.feab_gram_fp64(L.dptr(X), X.element_size(), n, MAX_SNAPSHOTS, L.dptr(G), L.dptr(ws), wbytes,
                               L.stream_ptr(dev))

@@ -678,6 +678,14 @@ def main():
     roof64 = spmv_roofline(op64, "fp64", args.spmv_reps, peak)
     for r in (roof, roof64):
         r["peak_source"] = f"MEASURED_PEAKS.json hbm_gbs (of {peak_kind})"
+    try:  # DRAM bytes of the same kernel from one ncu capture (profiles/)
+        tr = json.load(open(os.path.join(ROOT, "profiles", "dram_traffic.json")))
+        t = tr.get(f"cantilever {shape[0]}x{shape[1]}x{shape[2]}", {}).get("mixed")
+        if t:
+            roof["traffic"] = t["dram_bytes"]
+            roof["traffic_kernel"] = t["kernel"]
+    except (OSError, ValueError, KeyError):
+        pass
     e2e_ms, h2d, d2h = e2e_steps(c, "mixed", args.tol, args.e2e_steps, 1)
     e2e_ms = max_over_ranks(e2e_ms, world)
     cpu = None

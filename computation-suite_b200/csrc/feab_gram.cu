@@ -282,17 +282,23 @@ __global__ void __launch_bounds__(kThreadsG) k_gram_bf16x3(const float* __restri
   for (int j = 0; j < kCols; ++j) out[j] = acc[j];
 }
 
-// G[m][n] = sum over CTAs of part[cta][m][n] + part[cta][64+m][n]; then symmetrised.
-__global__ void k_gram_reduce(const double* __restrict__ part, int ctas, double* __restrict__ G) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+// G[m][n] = sum over CTAs of part[cta][m][n] + part[cta][64+m][n]; then symmetrised.  One warp
+// per entry: lane l sums CTAs l, l+32, ... in order, then a fixed shuffle tree (deterministic).
+constexpr int kReduceWarps = 8;
+
+__global__ void __launch_bounds__(32 * kReduceWarps) k_gram_reduce(const double* __restrict__ part, int ctas,
+                                                                   double* __restrict__ G) {
+  const int idx = blockIdx.x * kReduceWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (idx >= kCols * kCols) return;
   const int m = idx / kCols, nn = idx % kCols;
   double s = 0.0, t = 0.0;
-  for (int c = 0; c < ctas; ++c) {
-    s += part[((int64_t)c * 128 + m) * kCols + nn] + part[((int64_t)c * 128 + 64 + m) * kCols + nn];
-    t += part[((int64_t)c * 128 + nn) * kCols + m] + part[((int64_t)c * 128 + 64 + nn) * kCols + m];
+  for (int c = lane; c < ctas; c += 32) {
+    s += __ldg(part + ((int64_t)c * 128 + m) * kCols + nn) + __ldg(part + ((int64_t)c * 128 + 64 + m) * kCols + nn);
+    t += __ldg(part + ((int64_t)c * 128 + nn) * kCols + m) + __ldg(part + ((int64_t)c * 128 + 64 + nn) * kCols + m);
   }
-  G[idx] = 0.5 * (s + t);
+  s = warp_sum(s);
+  t = warp_sum(t);
+  if (lane == 0) G[idx] = 0.5 * (s + t);
 }
 
 // One-block cyclic Jacobi eigensolver for a symmetric k x k FP64 matrix (k <= 64), round-robin
@@ -472,17 +478,20 @@ __global__ void __launch_bounds__(kGThreads, 1) k_gram_fp64(const T* __restrict_
   for (int e = tid; e < kCols * kCols; e += kGThreads) part[(int64_t)blockIdx.x * kCols * kCols + e] = xs[e];
 }
 
-// G = sum over CTAs (fixed order) of part[cta], symmetrised.
-__global__ void k_gram_reduce64(const double* __restrict__ part, int ctas, double* __restrict__ G) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+// G = sum over CTAs of part[cta], symmetrised; one warp per entry as k_gram_reduce (deterministic).
+__global__ void __launch_bounds__(32 * kReduceWarps) k_gram_reduce64(const double* __restrict__ part, int ctas,
+                                                                     double* __restrict__ G) {
+  const int idx = blockIdx.x * kReduceWarps + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (idx >= kCols * kCols) return;
   const int m = idx / kCols, nn = idx % kCols;
   double s = 0.0, t = 0.0;
-  for (int c = 0; c < ctas; ++c) {
-    s += part[(int64_t)c * kCols * kCols + m * kCols + nn];
-    t += part[(int64_t)c * kCols * kCols + nn * kCols + m];
+  for (int c = lane; c < ctas; c += 32) {
+    s += __ldg(part + (int64_t)c * kCols * kCols + m * kCols + nn);
+    t += __ldg(part + (int64_t)c * kCols * kCols + nn * kCols + m);
   }
-  G[idx] = 0.5 * (s + t);
+  s = warp_sum(s);
+  t = warp_sum(t);
+  if (lane == 0) G[idx] = 0.5 * (s + t);
 }
 
 int gram_fp64_grid(int64_t n) {
@@ -515,7 +524,7 @@ extern "C" int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double
   FEAB_CUDA(cudaFuncSetAttribute(k_gram_bf16x3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   double* part = static_cast<double*>(workspace);
   k_gram_bf16x3<<<grid, kThreadsG, smem, s>>>(X, n, part, error_flag);
-  k_gram_reduce<<<(kCols * kCols + 255) / 256, 256, 0, s>>>(part, grid, G);
+  k_gram_reduce<<<(kCols * kCols + kReduceWarps - 1) / kReduceWarps, 32 * kReduceWarps, 0, s>>>(part, grid, G);
   count_launches(2);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;
@@ -529,7 +538,7 @@ extern "C" int32_t feab_gram_fp64(const void* X, int32_t x_bytes, int64_t n, int
   double* part = static_cast<double*>(workspace);
   if (x_bytes == 4) k_gram_fp64<float><<<grid, kGThreads, 0, s>>>(static_cast<const float*>(X), n, part);
   else k_gram_fp64<double><<<grid, kGThreads, 0, s>>>(static_cast<const double*>(X), n, part);
-  k_gram_reduce64<<<(kCols * kCols + 255) / 256, 256, 0, s>>>(part, grid, G);
+  k_gram_reduce64<<<(kCols * kCols + kReduceWarps - 1) / kReduceWarps, 32 * kReduceWarps, 0, s>>>(part, grid, G);
   count_launches(2);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;

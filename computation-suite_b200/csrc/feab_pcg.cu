@@ -426,6 +426,32 @@ __global__ void __launch_bounds__(kThreads, FEAB_SELL_MINB) k_step_a_sell(PcgArg
         part[0] += ri * ri;
       }
     });
+  } else if (FEAB_SELL_FUSED_P) {
+    // p_new = z + beta p_old formed inside the gathers (two gathers per column) and written for
+    // the lane's own rows into the other half of the p ping-pong; no separate P pass
+    const int pend = S->p_pending, psel = S->psel;
+    const double beta = S->beta;
+    const double* __restrict__ po = psel ? A.p1 : A.p0;
+    double* __restrict__ pn = psel ? A.p0 : A.p1;
+    const int nw = (gridDim.x * blockDim.x) >> 5;
+    for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < A.sell.n_slices; sl += nw) {
+      const SellLane L = sell_lane(A.sell, sl, lane);
+      double acc[3], xs[3];
+      if (pend)
+        sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc, xs);
+      else
+        sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(po + j); }, acc, xs);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k < L.f) {
+          const int i = L.r0 + k;
+          const double pi = pend ? A.z[i] + beta * po[i] : po[i];
+          if (pend) pn[i] = pi;
+          A.Ap[i] = acc[k];
+          part[0] += pi * acc[k];
+        }
+      }
+    }
   } else {
     const int nw = (gridDim.x * blockDim.x) >> 5;
     for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < A.sell.n_slices; sl += nw) {
@@ -447,6 +473,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_SELL_MINB) k_step_a_sell(PcgArg
     if (mode == kModeReliable && PREC != FEAB_PREC_FP64) {
       S->rr64 = tot[0];
     } else {
+      if (FEAB_SELL_FUSED_P && S->p_pending) S->psel ^= 1;
       S->p_pending = 0;
       S->pAp = tot[0];
       if (!(tot[0] > 0.0)) {  // p^T A p <= 0: A is not SPD (iterative_solvers.py:450-454)
@@ -813,7 +840,7 @@ int sell_grid(const PcgArgs& A) {
 
 template <int PREC>
 void launch_step_sell(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
-  k_step_p<<<gr.b, kThreads, 0, s>>>(A);
+  if (!FEAB_SELL_FUSED_P) k_step_p<<<gr.b, kThreads, 0, s>>>(A);
   k_step_a_sell<PREC><<<sell_grid(A), kThreads, 0, s>>>(A);
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
 }
@@ -862,7 +889,7 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
     if (fail(cudaGraphLaunch(exec, s))) break;
     if (fail(cudaEventRecord(ev[0], s))) break;
     launched = 1;
-    const uint64_t per_step = A.use_sell ? 3 : 2;
+    const uint64_t per_step = A.use_sell ? (FEAB_SELL_FUSED_P ? 2 : 3) : 2;
     count_launches(per_step * (uint64_t)chunk);
     while (true) {
       const bool more = launched < max_launch;

@@ -28,6 +28,11 @@
 #ifndef FEAB_SELL_STREAM
 #define FEAB_SELL_STREAM 1
 #endif
+// 1: the PCG forms p = z + beta p inside the sliced SpMV's gathers (two gathers per column)
+// instead of a separate pass.
+#ifndef FEAB_SELL_FUSED_P
+#define FEAB_SELL_FUSED_P 0
+#endif
 // Minimum resident 256-thread CTAs per SM for the sliced SpMV kernels (register budget).
 #ifndef FEAB_SELL_MINB
 #define FEAB_SELL_MINB 2

@@ -5,9 +5,10 @@
 // (batched_solve.py:105-164) applies one factorisation to many columns -- while the matrix is
 // read once per step for all columns of a problem (SpMM over the panel).
 //
-// One step is three kernels: P (P = Z + beta P for problems with a pending direction), A (SpMM
-// AP = K P and the per-column p.Ap, or the FP64 residual in a reliable step) and B (X, R, Z,
-// per-column r.r and r.z, convergence, beta).
+// One step is three kernels: P (P = M R + beta P for problems with a pending direction), A
+// (SpMM AP = K P and the per-column p.Ap, or the FP64 residual in a reliable step) and B (X, R,
+// per-column r.r and r.z, convergence, beta).  The preconditioned residual Z = M R (Jacobi) is
+// never stored: P and B form it from R and the inverse diagonal where they need it.
 //
 // Layout: vectors are row-major panels n x K (K = panel width, a power of two <= 64);
 // problem p owns a contiguous row range and a contiguous range of node row groups.  Work is
@@ -68,7 +69,7 @@ struct BArgs {
   const int32_t* prob_cols;
   const double* B;   // n x k
   double* X;         // n x k
-  double *R, *Z, *P0, *AP;
+  double *R, *P0, *AP;
   double* part;      // n_items x 2k
   ProbState* ps;
   ColState* cs;
@@ -114,15 +115,25 @@ constexpr int kUnroll = FEAB_BLOCK_UNROLL;
 #ifndef FEAB_BLOCK_VECB
 #define FEAB_BLOCK_VECB 1
 #endif
+// column pairs per thread and trip of the vector pass (loads in flight before any store)
+#ifndef FEAB_BLOCK_VECU
+#define FEAB_BLOCK_VECU 4
+#endif
+constexpr int kVecU = FEAB_BLOCK_VECU;
 // minimum resident CTAs per SM of the SpMM kernel (register budget)
 #ifndef FEAB_BLOCK_MINB
 #define FEAB_BLOCK_MINB 1
 #endif
 
-struct GroupStage {
+struct __align__(16) GroupStage {
   int col[kStageCols];
   double val[3][kStageCols];
 };
+// 1: with one sub-warp per warp (panels of 32 or more columns) the SpMM reads the staged
+// columns and values as 16-byte broadcasts (4 columns / 2 values per shared-memory load)
+#ifndef FEAB_BLOCK_VLDS
+#define FEAB_BLOCK_VLDS 1
+#endif
 
 // Panel column of accumulator q of lane-in-sub-warp cl: a 64-wide panel gives each lane two
 // adjacent columns (one 16-byte gather per panel row), narrower panels one column per lane.
@@ -211,6 +222,56 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
       }
     }
     __syncwarp();
+    if constexpr (MPW == 1 && FEAB_BLOCK_VLDS && kUnroll % 4 == 0) {
+      // m0 is a multiple of kUnroll, so the vector reads stay inside the kStageCols-entry stage
+      // (entries past nc are read but not used)
+      for (int m0 = 0; m0 < nc; m0 += kUnroll) {
+        unsigned t[kUnroll];
+        double xv[kUnroll][CPL];
+#pragma unroll
+        for (int u4 = 0; u4 < kUnroll / 4; ++u4) {
+          const int4 tq = *reinterpret_cast<const int4*>(&st.col[m0 + 4 * u4]);
+          t[4 * u4] = (unsigned)tq.x;
+          t[4 * u4 + 1] = (unsigned)tq.y;
+          t[4 * u4 + 2] = (unsigned)tq.z;
+          t[4 * u4 + 3] = (unsigned)tq.w;
+        }
+#pragma unroll
+        for (int u = 0; u < kUnroll; ++u) {
+          if (m0 + u < nc) {
+            gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), cl, xv[u]);
+          } else {
+#pragma unroll
+            for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;
+          }
+        }
+#pragma unroll
+        for (int u2 = 0; u2 < kUnroll / 2; ++u2) {
+          if (m0 + 2 * u2 >= nc) break;
+          const double2 w0 = *reinterpret_cast<const double2*>(&st.val[0][m0 + 2 * u2]);
+          const double2 w1 = *reinterpret_cast<const double2*>(&st.val[1][m0 + 2 * u2]);
+          const double2 w2 = *reinterpret_cast<const double2*>(&st.val[2][m0 + 2 * u2]);
+          // a column past nc has xv = 0 but a stale value: skip it rather than form 0 * stale
+          const bool two = m0 + 2 * u2 + 1 < nc;
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            const double d = xv[2 * u2][q];
+            acc[0][q] = fma(w0.x, d, acc[0][q]);
+            acc[1][q] = fma(w1.x, d, acc[1][q]);
+            acc[2][q] = fma(w2.x, d, acc[2][q]);
+          }
+          if (two) {
+#pragma unroll
+            for (int q = 0; q < CPL; ++q) {
+              const double d = xv[2 * u2 + 1][q];
+              acc[0][q] = fma(w0.y, d, acc[0][q]);
+              acc[1][q] = fma(w1.y, d, acc[1][q]);
+              acc[2][q] = fma(w2.y, d, acc[2][q]);
+            }
+          }
+        }
+      }
+    } else
     for (int m0 = sub; m0 < nc; m0 += MPW * kUnroll) {
       unsigned t[kUnroll];
       double xv[kUnroll][CPL];
@@ -263,7 +324,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
   }
 }
 
-// setup: R = B - 0 (x0 = 0), Z = M R, P = Z, per column ||b||, r.z; columns beyond the problem's
+// setup: R = B - 0 (x0 = 0), P = M R, per column ||b||, r.z; columns beyond the problem's
 // RHS count are inactive from the start.
 template <int K>
 __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
@@ -278,7 +339,6 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
       const double bi = A.B[idx];
       const double zi = A.dinv[i] * bi;
       A.R[idx] = bi;
-      A.Z[idx] = zi;
       A.P0[idx] = zi;
       A.X[idx] = 0.0;
       bb += bi * bi;
@@ -420,39 +480,65 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
   }
 }
 
-// Direction update P = Z + beta P (in place, per column beta; frozen columns have beta = 0, so
-// P = Z) for the problems whose new direction is pending.
+// Direction update P = M R + beta P (in place, per column beta; frozen columns have beta = 0,
+// so P = M R) for the problems whose new direction is pending.
 template <int K>
 __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
-  const int c = threadIdx.x % K;
   double* __restrict__ P0 = A.P0;
-  const double* __restrict__ Z = A.Z;
+  const double* __restrict__ R = A.R;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
     const ProbState P = A.ps[p];
     if (P.done || !P.pending) continue;
-    const double beta = A.cs[(int64_t)p * K + c].beta;
     const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
-    const int64_t e0 = (int64_t)r0 * K + threadIdx.x, e1 = (int64_t)r1 * K;
-    for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
-      double zv[4], pv[4];
+    if constexpr (K >= 2) {
+      // two adjacent columns per thread with 16-byte accesses, four pairs per trip
+      const int c2 = 2 * (threadIdx.x % (K / 2));
+      const double b0 = A.cs[(int64_t)p * K + c2].beta, b1 = A.cs[(int64_t)p * K + c2 + 1].beta;
+      const int64_t q0 = (int64_t)r0 * (K / 2) + threadIdx.x, q1 = (int64_t)r1 * (K / 2);
+      double2* __restrict__ P2 = reinterpret_cast<double2*>(P0);
+      const double2* __restrict__ R2 = reinterpret_cast<const double2*>(R);
+      for (int64_t q = q0; q < q1; q += 4 * kThreads) {
+        double2 rv[4], pv[4];
+        double dv[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int64_t e = idx + (int64_t)u * kThreads;
-        zv[u] = e < e1 ? Z[e] : 0.0;
-        pv[u] = e < e1 ? P0[e] : 0.0;
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = q + (int64_t)u * kThreads;
+          const bool ok = e < q1;
+          rv[u] = ok ? R2[e] : make_double2(0.0, 0.0);
+          pv[u] = ok ? P2[e] : make_double2(0.0, 0.0);
+          dv[u] = ok ? __ldg(A.dinv + e / (K / 2)) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = q + (int64_t)u * kThreads;
+          if (e < q1) P2[e] = make_double2(dv[u] * rv[u].x + b0 * pv[u].x, dv[u] * rv[u].y + b1 * pv[u].y);
+        }
       }
+    } else {
+      const double beta = A.cs[(int64_t)p].beta;
+      const int64_t e0 = (int64_t)r0 + threadIdx.x, e1 = (int64_t)r1;
+      for (int64_t idx = e0; idx < e1; idx += 4 * kThreads) {
+        double rv[4], pv[4], dv[4];
 #pragma unroll
-      for (int u = 0; u < 4; ++u) {
-        const int64_t e = idx + (int64_t)u * kThreads;
-        if (e < e1) P0[e] = zv[u] + beta * pv[u];
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = idx + (int64_t)u * kThreads;
+          rv[u] = e < e1 ? R[e] : 0.0;
+          pv[u] = e < e1 ? P0[e] : 0.0;
+          dv[u] = e < e1 ? __ldg(A.dinv + e) : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int64_t e = idx + (int64_t)u * kThreads;
+          if (e < e1) P0[e] = dv[u] * rv[u] + beta * pv[u];
+        }
       }
     }
   }
 }
 
-// Step B: X += alpha P, R -= alpha AP, Z = M R (CG) or Z = M R (reliable); per column r.r, r.z;
-// per-column convergence, beta, problem bookkeeping.
+// Step B: X += alpha P, R -= alpha AP (CG step; a reliable step leaves both); per column r.r
+// and r.z with z = M r formed on the fly; per-column convergence, beta, problem bookkeeping.
 template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
   __shared__ double sm[2][kThreads];
@@ -467,11 +553,10 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
     const double* __restrict__ pc = A.P0;
     double* __restrict__ X = A.X;
     double* __restrict__ R = A.R;
-    double* __restrict__ Z = A.Z;
     const double* __restrict__ AP = A.AP;
     const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
     if constexpr (K >= 2 && FEAB_BLOCK_VECB) {
-      // two adjacent columns c2, c2 + 1 per thread with 16-byte accesses, two pairs per trip,
+      // two adjacent columns c2, c2 + 1 per thread with 16-byte accesses, kVecU pairs per trip,
       // every load of the trip issued before any store
       const int c2 = 2 * (threadIdx.x % (K / 2));
       const double al0 = A.cs[(int64_t)p * K + c2].alpha, al1 = A.cs[(int64_t)p * K + c2 + 1].alpha;
@@ -481,12 +566,11 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
       const double2* __restrict__ AP2 = reinterpret_cast<const double2*>(AP);
       double2* __restrict__ X2 = reinterpret_cast<double2*>(X);
       double2* __restrict__ R2 = reinterpret_cast<double2*>(R);
-      double2* __restrict__ Z2 = reinterpret_cast<double2*>(Z);
-      for (int64_t q = q0; q < q1; q += 2 * kThreads) {
-        double2 xv[2], pv[2], rv[2], av[2];
-        double dv[2];
+      for (int64_t q = q0; q < q1; q += kVecU * kThreads) {
+        double2 xv[kVecU], pv[kVecU], rv[kVecU], av[kVecU];
+        double dv[kVecU];
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kVecU; ++u) {
           const int64_t e = q + (int64_t)u * kThreads;
           const bool ok = e < q1;
           rv[u] = ok ? R2[e] : make_double2(0.0, 0.0);
@@ -498,7 +582,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
           }
         }
 #pragma unroll
-        for (int u = 0; u < 2; ++u) {
+        for (int u = 0; u < kVecU; ++u) {
           const int64_t e = q + (int64_t)u * kThreads;
           if (e >= q1) break;
           double ri0 = rv[u].x, ri1 = rv[u].y;
@@ -509,7 +593,6 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
             R2[e] = make_double2(ri0, ri1);
           }
           const double zi0 = dv[u] * ri0, zi1 = dv[u] * ri1;
-          Z2[e] = make_double2(zi0, zi1);
           rr0 += ri0 * ri0;
           rr1 += ri1 * ri1;
           rz0 += ri0 * zi0;
@@ -564,7 +647,6 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
             R[e] = ri;
           }
           const double zi = dv[u] * ri;
-          Z[e] = zi;
           rr += ri * ri;
           rz += ri * zi;
         }
@@ -654,7 +736,7 @@ size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct BLayout {
   size_t total;
-  size_t o_R, o_Z, o_P0, o_AP, o_part, o_ps, o_cs, o_rem;
+  size_t o_R, o_P0, o_AP, o_part, o_ps, o_cs, o_rem;
 };
 
 BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
@@ -667,7 +749,6 @@ BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
   };
   const size_t panel = sizeof(double) * (size_t)n * (size_t)k;
   L.o_R = take(panel);
-  L.o_Z = take(panel);
   L.o_P0 = take(panel);
   L.o_AP = take(panel);
   L.o_part = take(sizeof(double) * 2 * (size_t)k * (size_t)n_items);
@@ -827,7 +908,6 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   A.B = B;
   A.X = X;
   A.R = reinterpret_cast<double*>(w + L.o_R);
-  A.Z = reinterpret_cast<double*>(w + L.o_Z);
   A.P0 = reinterpret_cast<double*>(w + L.o_P0);
   A.AP = reinterpret_cast<double*>(w + L.o_AP);
   A.part = reinterpret_cast<double*>(w + L.o_part);

@@ -63,6 +63,7 @@ class FESystem:
         self._K_full = None
         self._stiffness_args = None
         self.last_solve_info = None
+        self._bc_cache = None    # (frozenset of fixed DOFs, free, fixed, {device: (free_t, fixed_t)})
 
     # ------------------------------------------------------------------ device objects
     @property
@@ -190,11 +191,10 @@ class FESystem:
     def fix_dofs(self, node_ids, dof_indices, value=0.0):
         nodes = self._check_nodes(node_ids, "fix_dofs")
         dofs = self._check_local_dofs(dof_indices, "fix_dofs")
-        for n in nodes:
-            for k in dofs:
-                dof = self.npn * int(n) + int(k)
-                self.fixed_dofs.add(dof)
-                self.fixed_dof_values[dof] = float(value)
+        # node-major, the same insertion order as one loop over nodes then local DOFs
+        ids = (self.npn * nodes.astype(np.int64)[:, None] + dofs.astype(np.int64)[None, :]).reshape(-1).tolist()
+        self.fixed_dofs.update(ids)
+        self.fixed_dof_values.update(dict.fromkeys(ids, float(value)))
 
     def add_nodal_force(self, node_ids, dof_index, total_force):
         nodes = self._check_nodes(node_ids, "add_nodal_force")
@@ -212,25 +212,44 @@ class FESystem:
         shares = facet_load_shares_batch(np.asarray(self.mesh.nodes)[facets], traction * thickness, quad_order)
         np.add.at(self.F, self.npn * facets.reshape(-1) + dof_index, shares.reshape(-1))
 
+    def _bc_arrays(self):
+        """(free, fixed) DOF index arrays for the current fixed set, recomputed only when the set
+        changes (the set is compared by value, so direct edits of ``fixed_dofs`` are seen)."""
+        key = frozenset(self.fixed_dofs)
+        c = self._bc_cache
+        if c is None or c[0] != key:
+            fixed = np.fromiter(key, dtype=np.int64, count=len(key))
+            fixed.sort()
+            mask = np.ones(self.n_dof, dtype=bool)
+            mask[fixed] = False
+            c = self._bc_cache = (key, np.flatnonzero(mask), fixed.astype(int), {})
+        return c
+
+    def _bc_device_index(self):
+        """Device copies of the (free, fixed) index arrays for the current fixed set."""
+        c = self._bc_arrays()
+        dev = self.device
+        if dev not in c[3]:
+            c[3][dev] = (torch.as_tensor(c[1]).to(dev), torch.as_tensor(c[2]).to(dev))
+        return c[3][dev]
+
     @property
     def free_dofs(self):
-        mask = np.ones(self.n_dof, dtype=bool)
-        if self.fixed_dofs:
-            mask[np.fromiter(self.fixed_dofs, dtype=np.int64)] = False
-        return np.flatnonzero(mask)
+        return self._bc_arrays()[1].copy()
 
     @property
     def fixed_dofs_array(self):
-        return np.array(sorted(self.fixed_dofs), dtype=int)
+        return self._bc_arrays()[2].copy()
 
     def _fixed_dof_values_array(self, fixed):
-        return np.array([self.fixed_dof_values.get(int(d), 0.0) for d in fixed])
+        vals = self.fixed_dof_values
+        return np.fromiter((vals.get(d, 0.0) for d in np.asarray(fixed).tolist()), dtype=float, count=len(fixed))
 
     # ------------------------------------------------------------------ reduced operator
     def reduced_operator(self, want32=True):
         """K_ff for the current fixed set on the device (cached until K or the BCs change)."""
         self._require_stiffness("reduced_operator")
-        fixed = self.fixed_dofs_array
+        fixed = self._bc_arrays()[2]
         key = (self._ke_version, fixed.tobytes(), bool(want32))
         if self._op_cache is not None and self._op_cache[0] == key:
             return self._op_cache[1]
@@ -243,15 +262,14 @@ class FESystem:
     def _reduced_rhs(self, F=None):
         """F_f - K[free, fixed] u_fixed as a device vector (solver.py:1496-1511)."""
         Fv = self.F if F is None else np.asarray(F, dtype=float)
-        free = self.free_dofs
-        fixed = self.fixed_dofs_array
+        _, free, fixed, _ = self._bc_arrays()
         u_fixed = self._fixed_dof_values_array(fixed)
         Ff = torch.as_tensor(np.ascontiguousarray(Fv[free])).to(self.device)
         if fixed.size and np.any(u_fixed):
             v = np.zeros(self.n_dof)
             v[fixed] = u_fixed
             y = self.device_mesh.apply(self._ke, v)
-            Ff = Ff - y[torch.as_tensor(free).to(self.device)]
+            Ff = Ff - y[self._bc_device_index()[0]]
         return Ff
 
     @property
@@ -278,7 +296,7 @@ class FESystem:
     def solve_static_device(self, verbose=False, method=None, **method_kwargs):
         """solve_static, returning the full displacement vector as a device tensor."""
         self._require_stiffness("solve_static")
-        fixed = self.fixed_dofs_array
+        fixed = self._bc_arrays()[2]
         u_fixed = self._fixed_dof_values_array(fixed)
         if not np.any(self.F) and not np.any(u_fixed):
             warnings.warn("solve_static: the load vector F is all zeros and no non-zero displacement is "
@@ -314,10 +332,10 @@ class FESystem:
                                f"(final relative residual {info.relres:.3e} >= tol={tol:.1e}).")
         L.raise_for(info.status, "solve_static")
         U = torch.zeros(self.n_dof, dtype=torch.float64, device=self.device)
-        free_t = torch.as_tensor(self.free_dofs).to(self.device)
+        free_t, fixed_t = self._bc_device_index()
         U[free_t] = x
-        if fixed.size:
-            U[torch.as_tensor(fixed).to(self.device)] = torch.as_tensor(u_fixed).to(self.device)
+        if fixed.size and np.any(u_fixed):
+            U[fixed_t] = torch.as_tensor(u_fixed).to(self.device)
         if verbose:
             print(f"[feab200] n={op.n} nnz={op.nnz} precision={precision} iters={info.iters} "
                   f"relres={info.relres:.3e} reliable_updates={info.reliable_updates} "

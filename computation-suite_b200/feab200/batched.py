@@ -155,6 +155,15 @@ class ProblemBatch:
         self.cols = [F.shape[1] for F in self.loads]
         self.K = panel_width(max(self.cols))
         self.op = None
+        self._didx = None
+
+    def _device_index(self):
+        """Device int64 copies of (each free row's DOF within its own problem, its DOF in the
+        concatenated system), uploaded once."""
+        if self._didx is None:
+            local = self.free - 3 * np.repeat(self.node_offsets[:-1], np.diff(self.row_bounds))
+            self._didx = (torch.as_tensor(local).to(self.device), torch.as_tensor(self.free).to(self.device))
+        return self._didx
 
     def assemble(self):
         pat = self.dm.pattern(self.fixed)
@@ -163,13 +172,15 @@ class ProblemBatch:
         return self.op
 
     def rhs_panel(self):
-        n = len(self.free)
-        B = np.zeros((n, self.K))
+        """The (n, K) right-hand-side panel on the device: each problem's load columns are
+        uploaded as given and their free rows gathered on the device."""
+        local_t, _ = self._device_index()
+        B = torch.zeros((len(self.free), self.K), dtype=torch.float64, device=self.device)
         for p, F in enumerate(self.loads):
-            a, b = self.row_bounds[p], self.row_bounds[p + 1]
-            rows = self.free[a:b] - 3 * self.node_offsets[p]
-            B[a:b, : F.shape[1]] = F[rows]
-        return torch.as_tensor(B).to(self.device)
+            a, b = int(self.row_bounds[p]), int(self.row_bounds[p + 1])
+            Fd = torch.from_numpy(np.ascontiguousarray(F)).to(self.device)
+            B[a:b, : F.shape[1]] = Fd.index_select(0, local_t[a:b])
+        return B
 
     def solve(self, tol=1e-8, maxiter=None, precision="fp64", reliable_delta=0.1, chunk=16):
         """Returns ([U_p (n_dof_p, k_p) numpy], BatchResult)."""
@@ -177,13 +188,14 @@ class ProblemBatch:
             self.assemble()
         X, res = block_pcg(self.op, self.row_bounds, self.rhs_panel(), self.cols, tol=tol, maxiter=maxiter,
                            precision=precision, reliable_delta=reliable_delta, chunk=chunk)
-        Xh = X.cpu().numpy()
-        out = []
-        for p, F in enumerate(self.loads):
-            a, b = self.row_bounds[p], self.row_bounds[p + 1]
-            U = np.zeros((3 * self.sizes[p], F.shape[1]))
-            U[self.free[a:b] - 3 * self.node_offsets[p]] = Xh[a:b, : F.shape[1]]
-            out.append(U)
+        # scatter the free rows into the concatenated DOF vectors on the device (fixed DOFs stay 0),
+        # copy once, and hand out each problem's rows and load columns as views
+        _, free_t = self._device_index()
+        U = torch.zeros((3 * int(self.node_offsets[-1]), self.K), dtype=torch.float64, device=self.device)
+        U.index_copy_(0, free_t, X)
+        Uh = U.cpu().numpy()
+        out = [Uh[3 * int(self.node_offsets[p]): 3 * int(self.node_offsets[p + 1]), : F.shape[1]]
+               for p, F in enumerate(self.loads)]
         return out, res
 
 

@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spmv-reps", type=int, default=20)
-    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv"],
+    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery"],
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
@@ -611,6 +611,104 @@ def workload_spmv(args):
             "roofline_fp64": out["fp64"], "roofline_fp32_csr": out["fp32"], "pcg_probe_iters": iters}
 
 
+def recovery_bytes(n_nodes, n_elem):
+    """Algorithmic bytes of one feab_hex8_recover call with every output: the element kernel reads
+    the connectivity (32 B per element) and each node's coordinates and displacement once
+    (48 B per node), writes the 8 corner records (448 B per element) and the element stress and
+    von Mises (56 B per element); the node kernel reads the incidence lists (4 B per node +
+    32 B per element), the connectivity again, the corner records (448 B per element) and writes
+    the nodal stress and von Mises (56 B per node)."""
+    return n_elem * (32 + 448 + 56 + 32 + 32 + 448) + n_nodes * (48 + 4 + 56)
+
+
+def workload_recovery(args):
+    """Stress recovery on the 128x32x32 cantilever after an FP64 solve: nodal and element stress and
+    von Mises in one feab_hex8_recover call (kernel time, L2 flushed before each launch), the same
+    through FESystem.stress + von_mises from host arrays, and the oracle on the host cores."""
+    import torch
+    import oracle as O
+    from feab200 import _lib as L
+    from feab200.device import DeviceMesh, DeviceStatus, pcg_solve
+    c = build_workload(tuple(args.shape))
+    X, el = c.mesh.nodes, c.mesh.elements
+    dev = torch.device("cuda", torch.cuda.current_device())
+    dm = DeviceMesh(X, el, device=dev)
+    op = dm.assemble(dm.element_stiffness(c.D), dm.pattern(c.fixed))
+    x, info = pcg_solve(op, torch.as_tensor(c.F[c.free]).to(dev), tol=1e-10, precision="fp64")
+    u = torch.zeros(c.n_dof, dtype=torch.float64, device=dev)
+    u[torch.as_tensor(c.free).to(dev)] = x
+    N, E = len(X), len(el)
+    topo = dm.topology()
+    f64 = dict(dtype=torch.float64, device=dev)
+    nodal, nvm, elem, evm = (torch.empty((N, 6), **f64), torch.empty(N, **f64), torch.empty((E, 6), **f64),
+                             torch.empty(E, **f64))
+    sbytes = int(L.lib.feab_hex8_recover_scratch_bytes(E))
+    scratch = torch.empty(sbytes, dtype=torch.uint8, device=dev)
+    st = DeviceStatus(dev)
+    Dm = L.dmat(c.D)
+
+    def launch():
+        rc = L.lib.feab_hex8_recover(L.dptr(dm.coords), L.dptr(dm.conn), E, N, L.dptr(topo.inc_ptr),
+                                     L.dptr(topo.inc_elem), Dm, L.dptr(u), L.dptr(nodal), L.dptr(nvm), L.dptr(elem),
+                                     L.dptr(evm), L.dptr(scratch), sbytes, st.ptr(), dm.stream)
+        L.raise_for(rc, "recovery")
+
+    n0 = L.lib.feab_launch_count()
+    for _ in range(max(3, args.warmup)):
+        launch()
+    torch.cuda.synchronize()
+    st.check("recovery")
+    flush = L2Flush(dev)
+    times = []
+    for _ in range(max(1, args.steps) * 4):
+        flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        launch()
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b) * 1e-3)
+    launches = int(L.lib.feab_launch_count() - n0)
+    t = statistics.mean(times)
+    nbytes = recovery_bytes(N, E)
+    peak, kind = measured_peak()
+    # parity against the oracle on the same displacement
+    uh = u.cpu().numpy()
+    t0 = time.perf_counter()
+    s_ref, e_ref = O.recover(X, el, uh, c.D)
+    cpu_s = time.perf_counter() - t0
+    rel = lambda a, b: float(np.linalg.norm(a - b) / np.linalg.norm(b))  # noqa: E731
+    # through the public API from host arrays
+    import feab200
+    fs = feab200.FESystem(feab200.Mesh(nodes=X, elements=el), feab200.Hex8Solid3D(), sparse=True)
+    fs.assemble_stiffness(c.D)
+    fs.stress(uh)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(3):
+        S = fs.stress(uh)
+        V = fs.von_mises(uh)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / 3
+    return {"metric": f"hex8 stress recovery (nodal + element stress and von Mises), {'x'.join(map(str, args.shape))}",
+            "value": round(t * 1e6, 2), "unit": "us", "n_nodes": N, "n_elements": E,
+            "roofline": {"bound": "hbm", "achieved": round(nbytes / t / 1e9, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(nbytes / t / 1e9 / peak, 3), "bytes_per_launch": int(nbytes),
+                         "kernels": "k_recover_elements + k_recover_nodes (one feab_hex8_recover call)",
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})"},
+            "rel_err_vs_oracle": {"stress_nodes": rel(nodal.cpu().numpy(), s_ref),
+                                  "stress_elements": rel(elem.cpu().numpy(), e_ref),
+                                  "von_mises_nodes": rel(nvm.cpu().numpy(), O.von_mises(s_ref)),
+                                  "fesystem_stress": rel(S.nodal, s_ref),
+                                  "fesystem_von_mises": rel(np.asarray(V), O.von_mises(s_ref))},
+            "e2e": {"value": round(e2e_ms, 2), "unit": "ms",
+                    "path": "FESystem.stress + FESystem.von_mises from a host numpy displacement",
+                    "h2d_bytes_per_step": 2 * 3 * N * 8, "d2h_bytes_per_step": N * 6 * 8 + N * 8},
+            "cpu_baseline": {"value": round(cpu_s * 1e3, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "oracle recover (NumPy einsum, all host threads) on the whole mesh, stress nodal "
+                                       "+ element"},
+            "gpu_launches": launches, "timing": "CUDA events around each call, L2 flushed before each"}
+
+
 # ----------------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -619,7 +717,7 @@ def main():
     args.world, args.rank = world, rank
     if args.workload != "cantilever" and args.impl == "ours":
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
-              "gram": workload_gram, "spmv": workload_spmv}[args.workload]
+              "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})

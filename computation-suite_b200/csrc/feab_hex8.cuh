@@ -33,6 +33,25 @@ __device__ __forceinline__ void dshape(int k, double xi, double eta, double zeta
   dz = 0.125 * sz * (1.0 + xi * sx) * (1.0 + eta * se);
 }
 
+// Determinant and inverse of a 3x3 matrix by cofactors; returns det.
+__device__ __forceinline__ double invert3(const double (&J)[3][3], double (&inv)[3][3]) {
+  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
+  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
+  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
+  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
+  const double r = 1.0 / det;
+  inv[0][0] = c00 * r;
+  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
+  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
+  inv[1][0] = c01 * r;
+  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
+  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
+  inv[2][0] = c02 * r;
+  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
+  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
+  return det;
+}
+
 // J = dN @ X (J[i][j] = sum_k dN[i][k] X[k][j]), its determinant and inverse.
 // Returns det; inv = J^-1, so physical gradients are g_k = inv @ dN[:, k]
 // (np.linalg.solve(J, dN) in elements/solids.py:147).
@@ -50,21 +69,7 @@ __device__ __forceinline__ double jacobian_inverse(const double (&X)[8][3], doub
       J[2][j] += c * X[k][j];
     }
   }
-  const double c00 = J[1][1] * J[2][2] - J[1][2] * J[2][1];
-  const double c01 = J[1][2] * J[2][0] - J[1][0] * J[2][2];
-  const double c02 = J[1][0] * J[2][1] - J[1][1] * J[2][0];
-  const double det = J[0][0] * c00 + J[0][1] * c01 + J[0][2] * c02;
-  const double r = 1.0 / det;
-  inv[0][0] = c00 * r;
-  inv[0][1] = (J[0][2] * J[2][1] - J[0][1] * J[2][2]) * r;
-  inv[0][2] = (J[0][1] * J[1][2] - J[0][2] * J[1][1]) * r;
-  inv[1][0] = c01 * r;
-  inv[1][1] = (J[0][0] * J[2][2] - J[0][2] * J[2][0]) * r;
-  inv[1][2] = (J[0][2] * J[1][0] - J[0][0] * J[1][2]) * r;
-  inv[2][0] = c02 * r;
-  inv[2][1] = (J[0][1] * J[2][0] - J[0][0] * J[2][1]) * r;
-  inv[2][2] = (J[0][0] * J[1][1] - J[0][1] * J[1][0]) * r;
-  return det;
+  return invert3(J, inv);
 }
 
 // Packed upper-block index of node pair (a, b), a <= b: rows of the upper triangle in order.

@@ -1,7 +1,8 @@
 """feab200: the hex8 linear-elastic assembly + Jacobi-PCG path of fea_engine on B200 GPUs.
 
 Drop-in names (same meaning as in fea_engine): FESystem, Mesh, box_mesh, Material, D_solid3d,
-Hex8Solid3D, preconditioned_cg, jacobi_preconditioner, and the SIMP functions in ``topopt``.
+Hex8Solid3D, preconditioned_cg, jacobi_preconditioner, the SIMP functions in ``topopt`` and the
+strain / stress / von Mises / reaction recovery in ``recovery`` (FESystem.stress etc.).
 All compute runs in libfeab200.so (hand-written sm_100a CUDA); importing the package fails if
 that library is missing.
 """
@@ -14,8 +15,8 @@ from .mesh import Mesh, box_mesh
 from .solver import FESystem
 from .iterative_solvers import jacobi_preconditioner, preconditioned_cg
 from .batched import ProblemBatch, solve_static_batched
-from . import batched, cantilever, facet_loads, topopt  # noqa: F401
+from . import batched, cantilever, facet_loads, recovery, topopt  # noqa: F401
 
 __all__ = ["FESystem", "Mesh", "box_mesh", "Material", "D_solid3d", "Hex8Solid3D", "FEField", "DeviceMesh",
            "ReducedOperator", "SolveInfo", "pcg_solve", "preconditioned_cg", "jacobi_preconditioner",
-           "ProblemBatch", "solve_static_batched", "batched", "cantilever", "facet_loads", "topopt"]
+           "ProblemBatch", "solve_static_batched", "batched", "cantilever", "facet_loads", "recovery", "topopt"]

@@ -108,6 +108,8 @@ SIGNATURES = {
     "feab_gram_fp64": (_I32, [_P, _I32, _I64, _I32, _P, _P, _SZ, _P]),
     "feab_symeig_jacobi": (_I32, [_P, _I32, _P, _P, _I32, _P, _P]),
     "feab_hex8_simp_vjp": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _D, _P, _P, _P, _P, _P]),
+    "feab_hex8_recover_scratch_bytes": (_SZ, [_I64]),
+    "feab_hex8_recover": (_I32, [_P, _P, _I64, _I32, _P, _P, C.POINTER(_D), _P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
 }
 
 

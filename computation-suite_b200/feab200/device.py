@@ -299,6 +299,42 @@ class DeviceMesh:
         L.raise_for(rc, "hex8 apply")
         return y
 
+    def recover(self, u, D=None, nodal=True, elements=False, von_mises=False, status=None):
+        """Strain (D is None) or stress (D given) recovered from the full displacement vector u
+        (3 n_nodes) by the lumped L2 projection of the Gauss-point values to the nodes
+        (recovery.py:196-334).  Returns a dict of device tensors: "nodal" (n_nodes, 6),
+        "elements" (n_elem, 6), and with von_mises (stress only) "nodal_vm" (n_nodes,) and
+        "elements_vm" (n_elem,), for the parts asked for."""
+        if von_mises and D is None:
+            raise ValueError("von Mises recovery needs the constitutive matrix D")
+        topo = self.topology()
+        dev = self.device
+        st = status or DeviceStatus(dev)
+        u = torch.as_tensor(u, dtype=torch.float64).to(dev).contiguous()
+        if u.shape != (3 * self.n_nodes,):
+            raise ValueError(f"expected a displacement vector of length {3 * self.n_nodes}, got {tuple(u.shape)}")
+        out = {}
+        f64 = dict(dtype=torch.float64, device=dev)
+        if nodal:
+            out["nodal"] = torch.empty((self.n_nodes, 6), **f64)
+        if elements:
+            out["elements"] = torch.empty((self.n_elem, 6), **f64)
+        if von_mises and nodal:
+            out["nodal_vm"] = torch.empty(self.n_nodes, **f64)
+        if von_mises and elements:
+            out["elements_vm"] = torch.empty(self.n_elem, **f64)
+        sbytes = int(L.lib.feab_hex8_recover_scratch_bytes(self.n_elem))
+        scratch = torch.empty(max(sbytes, 1), dtype=torch.uint8, device=dev)
+        rc = L.lib.feab_hex8_recover(L.dptr(self.coords), L.dptr(self.conn), self.n_elem, self.n_nodes,
+                                     L.dptr(topo.inc_ptr), L.dptr(topo.inc_elem),
+                                     None if D is None else L.dmat(D), L.dptr(u), L.dptr(out.get("nodal")),
+                                     L.dptr(out.get("nodal_vm")), L.dptr(out.get("elements")),
+                                     L.dptr(out.get("elements_vm")), L.dptr(scratch), sbytes, st.ptr(), self.stream)
+        L.raise_for(rc, "strain/stress recovery")
+        if status is None:
+            st.check("strain/stress recovery")
+        return out
+
     def simp_vjp(self, D_unit, rho, penal, rho_min, u, lam=None, status=None):
         """-p (1-rho_min) rho^(p-1) lam_e^T K0_e u_e per element (lam = u: dC/drho)."""
         st = status or DeviceStatus(self.device)

@@ -288,6 +288,37 @@ class FESystem:
         return FEField(data, n_nodes=len(self.mesh.nodes), dofs_per_node=3, dof_names=self.dof_names, label=label,
                        mesh=self.mesh)
 
+    # ------------------------------------------------------------------ derived results (recovery.py)
+    def stress(self, U=None, D=None, at="nodes", vectorized=True, backend="numpy", device="cpu"):
+        """Stress components as an FEField (``at="elements"``: element averages), solver.py:413-418."""
+        from . import recovery
+        return recovery.stress(self, self.solve_static() if U is None else U, D, at, vectorized, backend, device)
+
+    def strain(self, U=None, at="nodes", vectorized=True, backend="numpy", device="cpu"):
+        """Strain components (engineering shear), solver.py:420-423."""
+        from . import recovery
+        return recovery.strain(self, self.solve_static() if U is None else U, at, vectorized, backend, device)
+
+    def von_mises(self, U=None, D=None, plane="stress", nu=None, at="nodes", vectorized=True, backend="numpy",
+                  device="cpu"):
+        """Von Mises stress as a scalar FEField, solver.py:425-430."""
+        from . import recovery
+        return recovery.von_mises(self, self.solve_static() if U is None else U, D, plane, nu, at, vectorized,
+                                  backend, device)
+
+    def stress_tensor(self, U, D=None, device="cpu", at="nodes"):
+        from . import recovery
+        return recovery.stress_tensor(self, U, D, device, at)
+
+    def von_mises_tensor(self, U, D=None, device="cpu", plane="stress", nu=None, at="nodes"):
+        from . import recovery
+        return recovery.von_mises_tensor(self, U, D, device, plane, nu, at)
+
+    def reactions(self, U=None):
+        """Support reactions K U - F at the constrained DOFs, solver.py:442-445."""
+        from . import recovery
+        return recovery.reactions(self, U)
+
     # ------------------------------------------------------------------ solve
     def solve_static(self, verbose=False, method=None, **method_kwargs):
         U = self.solve_static_device(verbose=verbose, method=method, **method_kwargs)

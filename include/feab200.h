@@ -343,6 +343,29 @@ int32_t feab_hex8_simp_vjp(const double* coords, const int32_t* conn, int64_t n_
                            const double* u, const double* lam, double* out,
                            feab_device_status* status, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- strain / stress recovery
+ * Replaces recovery._recover / stress / strain / von_mises for Hex8 blocks
+ * (fea_engine/src/fea_engine/recovery.py:196-227 _block_batched, :258-334 _recover,
+ * :365-420 stress / strain / _mises / von_mises; FESystem.stress / strain / von_mises,
+ * solver.py:413-430).  At the 2x2x2 Gauss points val = D B u (D_host != NULL: stress) or
+ * B u (D_host == NULL: engineering strain), Voigt order xx, yy, zz, xy, yz, xz.
+ * nodal (n_nodes x 6): lumped L2 projection to the corners,
+ *   sum_e sum_q N_a |detJ| w val / sum_e sum_q N_a |detJ| w, summed over the node's elements in
+ *   ascending element order (nodes with no element get 0);
+ * elem (n_elem x 6): sum_q |detJ| w val / sum_q |detJ| w;
+ * nodal_vm / elem_vm: the von Mises stress of those (stress only).  Any of the four outputs
+ * may be NULL (not all).  u: 3*n_nodes.  inc_ptr / inc_elem: feab_node_incidence.  scratch:
+ * feab_hex8_recover_scratch_bytes(n_elem) bytes of device memory (8 doubles per element
+ * corner).  conn, nodal and scratch must be 16-byte aligned.  Asynchronous on the stream; a
+ * degenerate element sets status. */
+size_t feab_hex8_recover_scratch_bytes(int64_t n_elem);
+
+int32_t feab_hex8_recover(const double* coords, const int32_t* conn, int64_t n_elem, int32_t n_nodes,
+                          const int32_t* inc_ptr, const int32_t* inc_elem, const double* D_host,
+                          const double* u, double* nodal, double* nodal_vm, double* elem,
+                          double* elem_vm, void* scratch, size_t scratch_bytes,
+                          feab_device_status* status, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,6 +20,7 @@ __all__ = [
     "free_dofs", "quad4_shape_and_derivs", "HEX8_FACES", "facet_load_shares", "facet_mass",
     "jacobi_inverse_diagonal", "preconditioned_cg", "simp_scale", "simp_scale_grad",
     "compliance_sensitivity_closed_form", "pod_singular_values", "element_strain_energy_density",
+    "recover", "von_mises", "reactions",
 ]
 
 
@@ -333,6 +334,55 @@ def compliance_sensitivity_closed_form(ke_unit, conn, u_full, rho, p, rho_min, d
     u_e = np.asarray(u_full)[g]
     quad = np.einsum("ei,eij,ej->e", u_e, ke_unit, u_e)
     return -simp_scale_grad(rho, p, rho_min) * quad
+
+
+# ----------------------------------------------------------------------------- recovery
+def recover(nodes, conn, U, D=None):
+    """Strain (D is None) or stress (D given) of hex8 elements, as recovery._recover for one
+    Hex8 block (fea_engine/src/fea_engine/recovery.py:196-227 and :258-334): at each Gauss point
+    val = [D] B u_e; numE[e, a] += |detJ| w N_a val, denE[e, a] += |detJ| w N_a; nodal =
+    sum over elements (np.add.at over the connectivity) of numE / denE (0 where denE is 0);
+    elem = sum_q |detJ| w val / sum_q |detJ| w.  Returns (nodal (N, 6), elem (E, 6))."""
+    nodes = np.asarray(nodes, dtype=float)
+    conn = np.asarray(conn)
+    U = np.asarray(U, dtype=float)
+    X = nodes[conn]
+    ue = U[global_dofs(conn)]
+    E = len(conn)
+    numE, denE = np.zeros((E, 8, 6)), np.zeros((E, 8))
+    acc, vol = np.zeros((E, 6)), np.zeros(E)
+    pts, _ = _gauss_product_3d(2)
+    for (w, detJ, dN_g), p in zip(_gauss_geometry(X), pts):
+        N, _ = hex8_shape_and_derivs(*p)
+        val = np.einsum("esm,em->es", _b_matrices(dN_g), ue)
+        if D is not None:
+            val = np.einsum("st,et->es", np.asarray(D, dtype=float), val)
+        wt = np.abs(detJ) * w
+        numE += np.einsum("e,c,es->ecs", wt, N, val)
+        denE += np.einsum("e,c->ec", wt, N)
+        acc += wt[:, None] * val
+        vol += wt
+    num, den = np.zeros((len(nodes), 6)), np.zeros(len(nodes))
+    np.add.at(num, conn, numE)
+    np.add.at(den, conn, denE)
+    nodal = np.divide(num, den[:, None], out=np.zeros_like(num), where=den[:, None] > 0)
+    return nodal, acc / vol[:, None]
+
+
+def von_mises(s):
+    """3-D von Mises stress of Voigt rows [xx, yy, zz, xy, yz, xz] (recovery.py:386-394)."""
+    s = np.asarray(s, dtype=float)
+    sxx, syy, szz, sxy, syz, sxz = (s[..., j] for j in range(6))
+    return np.sqrt(0.5 * ((sxx - syy) ** 2 + (syy - szz) ** 2 + (szz - sxx) ** 2)
+                   + 3.0 * (sxy ** 2 + syz ** 2 + sxz ** 2))
+
+
+def reactions(K, U, F, fixed):
+    """R = K U - F at the constrained DOFs, zero elsewhere (recovery.py:422-440)."""
+    r = np.asarray(K @ np.asarray(U, dtype=float)).ravel() - np.asarray(F, dtype=float).ravel()
+    out = np.zeros_like(r)
+    out[np.asarray(fixed)] = r[np.asarray(fixed)]
+    return out
 
 
 # ----------------------------------------------------------------------------- POD

@@ -26,6 +26,8 @@ facets.npz             consistent facet load shares / facet mass of 5 distorted 
 simp_6x3x3.npz         SIMP compliance: densities, forward solution, closed-form dc, the
                        torch-adjoint dc and central finite differences at 4 elements.
 pod_small.npz          singular values of a 400x12 snapshot matrix from PodBasis.fit.
+recovery_20x4x4.npz    the cantilever_20x4x4 system at its SuperLU displacement: FESystem.stress /
+                       strain / von_mises at the nodes and per element, and reactions.
 """
 from __future__ import annotations
 
@@ -54,14 +56,13 @@ def jitter(nodes, h, amp, seed):
     return X
 
 
-def cantilever_20x4x4():
+def _cantilever_20x4x4_system():
+    """The jittered 20x4x4 FESystem, clamped and loaded: (fs, mesh, D, facets)."""
     from fea_engine.mesh import box_mesh, Mesh
     from fea_engine.elements.solids import Hex8Solid3D
     from fea_engine.material import Material, D_solid3d
     from fea_engine.solver import FESystem
-    from fea_engine import facet_loads, iterative_solvers
-    from fea_engine.vectorized_assembly import scatter_global_stiffness, tensorized_element_stiffness
-    from fea_engine.mesh_transform import MeshTransformation
+    from fea_engine import facet_loads
 
     Lx, Ly, Lz, nx, ny, nz = 2.0, 0.4, 0.4, 20, 4, 4
     base = box_mesh(Lx, Ly, Lz, nx, ny, nz)
@@ -80,6 +81,17 @@ def cantilever_20x4x4():
             if all(n in tip for n in f):
                 facets.append(f)
     fs.add_consistent_facet_load(elem, facets, 2, -1.0e6)
+    return fs, mesh, D, facets
+
+
+def cantilever_20x4x4():
+    from fea_engine.elements.solids import Hex8Solid3D
+    from fea_engine import iterative_solvers
+    from fea_engine.vectorized_assembly import scatter_global_stiffness, tensorized_element_stiffness
+    from fea_engine.mesh_transform import MeshTransformation
+
+    fs, mesh, D, facets = _cantilever_20x4x4_system()
+    nodes, elem = mesh.nodes, Hex8Solid3D()
     rs = fs.form_linear_system()
     Kff = rs.K.tocsr()
     U_lu = np.asarray(fs.solve_static())
@@ -195,6 +207,20 @@ def simp_6x3x3():
                 compliance=np.float64(topopt.compliance(F, u)))
 
 
+def recovery_20x4x4():
+    """FESystem.stress / strain / von_mises (nodes and elements) and reactions of the jittered
+    20x4x4 cantilever at its SuperLU displacement (recovery.py through solver.py:413-445)."""
+    fs, mesh, D, _ = _cantilever_20x4x4_system()
+    U = np.asarray(fs.solve_static())
+    n = len(mesh.nodes)
+    return dict(nodes=np.asarray(mesh.nodes), elements=np.asarray(mesh.elements, dtype=np.int64), D=D, U=U,
+                F=np.asarray(fs.F), fixed=np.asarray(fs.fixed_dofs_array),
+                stress_nodes=np.asarray(fs.stress(U)).reshape(n, 6), stress_elements=np.asarray(fs.stress(U, at="elements")),
+                strain_nodes=np.asarray(fs.strain(U)).reshape(n, 6), strain_elements=np.asarray(fs.strain(U, at="elements")),
+                von_mises_nodes=np.asarray(fs.von_mises(U)), von_mises_elements=np.asarray(fs.von_mises(U, at="elements")),
+                reactions=np.asarray(fs.reactions(U)))
+
+
 def pod_small():
     from rom_engine.pod import PodBasis
     rng = np.random.default_rng(3)
@@ -208,11 +234,14 @@ def pod_small():
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", required=True)
+    ap.add_argument("--only", nargs="*", default=None, help="fixture names to write (default: all)")
     args = ap.parse_args()
     _import_reference(args.reference)
     for name, fn in [("cantilever_20x4x4", cantilever_20x4x4), ("pattern_4x3x2", pattern_4x3x2),
                      ("ke_distorted", ke_distorted), ("facets", facets), ("simp_6x3x3", simp_6x3x3),
-                     ("pod_small", pod_small)]:
+                     ("pod_small", pod_small), ("recovery_20x4x4", recovery_20x4x4)]:
+        if args.only and name not in args.only:
+            continue
         data = fn()
         path = os.path.join(HERE, name + ".npz")
         np.savez_compressed(path, **data)

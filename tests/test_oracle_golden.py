@@ -100,3 +100,23 @@ def test_pod_singular_values_match_reference(golden):
     g = golden("pod_small")
     s = O.pod_singular_values(g["X"])
     assert np.abs(s - g["singular_values"]).max() / g["singular_values"][0] < 1e-14
+
+
+def _relnorm(a, b):
+    return np.linalg.norm(np.asarray(a) - np.asarray(b)) / np.linalg.norm(np.asarray(b))
+
+
+def test_recovery_matches_reference(golden):
+    g = golden("recovery_20x4x4")
+    X, el, U, D = g["nodes"], g["elements"], g["U"], g["D"]
+    s_nodes, s_elem = O.recover(X, el, U, D)
+    e_nodes, e_elem = O.recover(X, el, U)
+    assert _relnorm(s_nodes, g["stress_nodes"]) < 1e-13 and _relnorm(s_elem, g["stress_elements"]) < 1e-13
+    assert _relnorm(e_nodes, g["strain_nodes"]) < 1e-13 and _relnorm(e_elem, g["strain_elements"]) < 1e-13
+    assert _relnorm(O.von_mises(s_nodes), g["von_mises_nodes"]) < 1e-13
+    assert _relnorm(O.von_mises(s_elem), g["von_mises_elements"]) < 1e-13
+    K = O.structural_csr(O.hex8_element_stiffness(X[el], D), el, 3 * len(X))
+    R = O.reactions(K, U, g["F"], g["fixed"])
+    assert _relnorm(R, g["reactions"]) < 1e-9
+    # the reactions balance the applied load (z: the -1e6 Pa traction on the 0.16 m^2 tip face)
+    assert abs(R[2::3].sum() - 1.6e5) < 1e-6 * 1.6e5

@@ -48,7 +48,8 @@ def parse():
     ap.add_argument("--cpu-iters", type=int, default=20, help="PCG iterations timed for the CPU baseline")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spmv-reps", type=int, default=20)
-    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery"],
+    ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery",
+                                           "simp_oc"],
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
@@ -709,6 +710,66 @@ def workload_recovery(args):
             "gpu_launches": launches, "timing": "CUDA events around each call, L2 flushed before each"}
 
 
+def workload_simp_oc(args):
+    """The SIMP optimality-criteria loop on the 96x32x32 cantilever (E0 = 1, unit tip load,
+    vf 0.4, p 3, rho_min 1e-3, move 0.2, filter radius 1.5 element lengths): time per iteration
+    of topopt.topology_optimize_compliance (assembly, PCG to 1e-9, dC/drho, filter, OC), and the
+    filter build, filter apply and OC update alone; the oracle's loop on a 24x8x8 mesh stands
+    in for the CPU (its dense filter matrix does not fit at 98,304 elements)."""
+    import torch
+    import feab200
+    import oracle as O
+    from feab200 import cantilever, topopt
+    c = cantilever.simp_cantilever(96, 32, 32)
+    mesh = feab200.Mesh(nodes=c.mesh.nodes, elements=c.mesh.elements)
+    fs = feab200.FESystem(mesh, feab200.Hex8Solid3D())
+    fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+    radius = 1.5 * 2.0 / 96
+    kw = dict(p=3.0, rho_min=1e-3, move=0.2, filter_radius=radius, pcg_tol=1e-9)
+    topopt.topology_optimize_compliance(fs, c.D, c.F, 0.4, n_iter=2, **kw)            # warm-up
+    n_it = max(4, 2 * args.steps)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    res = topopt.topology_optimize_compliance(fs, c.D, c.F, 0.4, n_iter=n_it, tol=0.0, **kw)
+    torch.cuda.synchronize()
+    ms_iter = (time.perf_counter() - t0) * 1e3 / len(res["compliance_history"])
+    dm = fs.device_mesh
+    cent = topopt.element_centroids(dm)
+
+    def ev(fn, reps=5):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        for _ in range(reps):
+            out = fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps, out
+
+    build_ms, H = ev(lambda: topopt.build_filter_weights(cent, radius), 2)
+    rho = torch.as_tensor(res["rho"]).to(dm.device)
+    dc = -torch.rand(dm.n_elem, dtype=torch.float64, device=dm.device)
+    filt_ms, _ = ev(lambda: topopt.apply_sensitivity_filter(H, rho, dc))
+    oc_ms, _ = ev(lambda: topopt._oc_device(rho, dc, 0.4, 0.2, 1e-3, 1.0, 1e-4, 100))
+    # CPU: the oracle's loop (dense filter, sparse direct solves) on 24x8x8
+    cs = cantilever.simp_cantilever(24, 8, 8)
+    t0 = time.perf_counter()
+    _, hist_cpu, _ = O.topology_optimize_compliance(cs.mesh.nodes, cs.mesh.elements, cs.D, cs.fixed, cs.F, 0.4, p=3.0,
+                                                    rho_min=1e-3, move=0.2, n_iter=3, filter_radius=1.5 * 2.0 / 24,
+                                                    tol=0.0)
+    cpu_ms = (time.perf_counter() - t0) * 1e3 / len(hist_cpu)
+    h = res["compliance_history"]
+    return {"metric": "SIMP optimality-criteria iteration time (assemble + PCG + dC/drho + filter + OC), 96x32x32 hex8",
+            "value": round(ms_iter, 2), "unit": "ms", "iterations_timed": len(h), "n_elements": dm.n_elem,
+            "filter_nnz": H.nnz, "filter_build_ms": round(build_ms, 3), "filter_apply_ms": round(filt_ms, 4),
+            "oc_update_ms": round(oc_ms, 4), "compliance_first_last": [h[0], h[-1]],
+            "volume_fraction_final": float(np.mean(res["rho"])),
+            "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms per iteration", "cores": os.cpu_count(),
+                             "kind": "port", "sample": "oracle loop (dense filter, SciPy sparse direct solve) on "
+                                                       "24x8x8, 3 iterations"}}
+
+
 # ----------------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -717,7 +778,8 @@ def main():
     args.world, args.rank = world, rank
     if args.workload != "cantilever" and args.impl == "ours":
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
-              "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery}[args.workload]
+              "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery,
+              "simp_oc": workload_simp_oc}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})

@@ -108,6 +108,12 @@ SIGNATURES = {
     "feab_gram_fp64": (_I32, [_P, _I32, _I64, _I32, _P, _P, _SZ, _P]),
     "feab_symeig_jacobi": (_I32, [_P, _I32, _P, _P, _I32, _P, _P]),
     "feab_hex8_simp_vjp": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _D, _P, _P, _P, _P, _P]),
+    "feab_element_centroids": (_I32, [_P, _P, _I64, _P, _P]),
+    "feab_filter_scratch_bytes": (_SZ, [_I64]),
+    "feab_filter_build": (_I32, [_P, _I64, _D, _P, _P, _P, _P, C.POINTER(_I64), _P, _SZ, _P]),
+    "feab_filter_apply": (_I32, [_P, _P, _P, _P, _I64, _P, _P, _D, _P, _P]),
+    "feab_oc_workspace_bytes": (_SZ, [_I64]),
+    "feab_oc_update": (_I32, [_P, _P, _I64, _D, _D, _D, _D, _D, _I32, _P, _P, _P, _SZ, _P]),
     "feab_hex8_recover_scratch_bytes": (_SZ, [_I64]),
     "feab_hex8_recover": (_I32, [_P, _P, _I64, _I32, _P, _P, C.POINTER(_D), _P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
 }

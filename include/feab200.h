@@ -343,6 +343,48 @@ int32_t feab_hex8_simp_vjp(const double* coords, const int32_t* conn, int64_t n_
                            const double* u, const double* lam, double* out,
                            feab_device_status* status, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- SIMP optimality-criteria loop
+ * The steps of topology_optimize_compliance (fea_engine/src/fea_engine/topopt.py:298-379) after
+ * the solve and dC/drho (feab_pcg_solve, feab_hex8_simp_vjp).
+ *
+ * feab_element_centroids: centroids (n_elem x 3) = mean of the 8 corner coordinates
+ * (mesh.nodes[conn].mean(axis=1), topopt.py:352).
+ *
+ * feab_filter_build: the filter weights H[e, j] = max(0, radius - |c_e - c_j|) of
+ * build_filter_weights (topopt.py:235-243) as a CSR over elements (columns ascending, only the
+ * positive entries), with rowsum[e] = sum_j H[e, j].  Two phases: with idx == NULL it counts,
+ * writes ptr (n_elem + 1) and *nnz_out (host) and synchronises (scratch:
+ * feab_filter_scratch_bytes); with idx != NULL it fills idx / w (nnz) and rowsum (n_elem),
+ * asynchronously (scratch unused).  Every pair of centroids is compared once per phase. */
+int32_t feab_element_centroids(const double* coords, const int32_t* conn, int64_t n_elem, double* centroids,
+                               cudaStream_t stream);
+
+size_t feab_filter_scratch_bytes(int64_t n_elem);
+
+int32_t feab_filter_build(const double* centroids, int64_t n_elem, double radius, int32_t* ptr, int32_t* idx,
+                          double* w, double* rowsum, int64_t* nnz_out, void* scratch, size_t scratch_bytes,
+                          cudaStream_t stream);
+
+/* out[e] = sum_j H[e, j] rho_j dc_j / max(max(rho_e, eps) rowsum[e], eps)
+ * (apply_sensitivity_filter, topopt.py:246-253).  out must not alias rho or dc. */
+int32_t feab_filter_apply(const int32_t* ptr, const int32_t* idx, const double* w, const double* rowsum,
+                          int64_t n_elem, const double* rho, const double* dc, double eps, double* out,
+                          cudaStream_t stream);
+
+/* oc_update (topopt.py:259-295): dc clipped to <= -1e-12; the bracket [1e-12, l2] on the volume
+ * multiplier is doubled (at most 60 times) until mean(rho_try) <= volume_fraction, then bisected
+ * until (l2 - l1) < bisection_tol * max(l2, 1) or max_bisection_iter steps, with
+ * rho_try = clip(clip(rho sqrt(-dc / l), rho - move, rho + move), rho_min_bound, rho_max_bound).
+ * rho_new receives the last bisection step's densities and *max_change (device double)
+ * max |rho_new - rho|.  Runs on the device with no host synchronisation (a fixed sequence of
+ * step kernels that return at once after convergence); workspace: feab_oc_workspace_bytes. */
+size_t feab_oc_workspace_bytes(int64_t n_elem);
+
+int32_t feab_oc_update(const double* rho, const double* dc, int64_t n_elem, double volume_fraction, double move,
+                       double rho_min_bound, double rho_max_bound, double bisection_tol,
+                       int32_t max_bisection_iter, double* rho_new, double* max_change, void* workspace,
+                       size_t workspace_bytes, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- strain / stress recovery
  * Replaces recovery._recover / stress / strain / von_mises for Hex8 blocks
  * (fea_engine/src/fea_engine/recovery.py:196-227 _block_batched, :258-334 _recover,

@@ -13,6 +13,7 @@ from __future__ import annotations
 
 import numpy as np
 import scipy.sparse as sp
+import scipy.sparse.linalg as spla
 
 __all__ = [
     "gauss_legendre", "box_mesh", "perturb_interior", "D_solid3d", "hex8_shape_and_derivs",
@@ -20,7 +21,8 @@ __all__ = [
     "free_dofs", "quad4_shape_and_derivs", "HEX8_FACES", "facet_load_shares", "facet_mass",
     "jacobi_inverse_diagonal", "preconditioned_cg", "simp_scale", "simp_scale_grad",
     "compliance_sensitivity_closed_form", "pod_singular_values", "element_strain_energy_density",
-    "recover", "von_mises", "reactions",
+    "recover", "von_mises", "reactions", "build_filter_weights", "apply_sensitivity_filter", "oc_update",
+    "topology_optimize_compliance",
 ]
 
 
@@ -334,6 +336,80 @@ def compliance_sensitivity_closed_form(ke_unit, conn, u_full, rho, p, rho_min, d
     u_e = np.asarray(u_full)[g]
     quad = np.einsum("ei,eij,ej->e", u_e, ke_unit, u_e)
     return -simp_scale_grad(rho, p, rho_min) * quad
+
+
+# ----------------------------------------------------------------------------- SIMP OC loop
+def build_filter_weights(centroids, radius):
+    """Dense H[e, j] = max(0, radius - |c_e - c_j|) (topopt.py:235-243)."""
+    c = np.asarray(centroids, dtype=float)
+    d = np.sqrt(np.sum((c[:, None, :] - c[None, :, :]) ** 2, axis=-1))
+    return np.maximum(0.0, radius - d)
+
+
+def apply_sensitivity_filter(H, rho, dc, eps=1e-9):
+    """H (rho dc) / max(max(rho, eps) H 1, eps) (topopt.py:246-253)."""
+    rho, dc = np.asarray(rho, dtype=float), np.asarray(dc, dtype=float)
+    return (H @ (rho * dc)) / np.maximum(np.maximum(rho, eps) * H.sum(axis=1), eps)
+
+
+def oc_update(rho, dc, volume_fraction, move=0.2, rho_min_bound=1e-3, rho_max_bound=1.0, bisection_tol=1e-4,
+              max_bisection_iter=100):
+    """Optimality-criteria update with an expanding bracket, then bisection, on the volume
+    multiplier (topopt.py:259-295)."""
+    rho = np.asarray(rho, dtype=float)
+    dc = np.minimum(np.asarray(dc, dtype=float), -1e-12)
+
+    def trial(lam):
+        t = np.clip(rho * np.sqrt(-dc / lam), rho - move, rho + move)
+        return np.clip(t, rho_min_bound, rho_max_bound)
+
+    lo, hi = 1e-12, 1.0
+    for _ in range(60):
+        if trial(hi).mean() <= volume_fraction:
+            break
+        hi *= 2.0
+    new = None
+    for _ in range(max_bisection_iter):
+        mid = 0.5 * (lo + hi)
+        new = trial(mid)
+        if new.mean() > volume_fraction:
+            lo = mid
+        else:
+            hi = mid
+        if hi - lo < bisection_tol * max(hi, 1.0):
+            break
+    return new
+
+
+def topology_optimize_compliance(nodes, conn, D, fixed, F_ext, volume_fraction, p=3.0, rho_min=1e-3, move=0.2,
+                                 n_iter=50, filter_radius=None, tol=1e-3):
+    """SIMP loop with the closed-form sensitivity (topopt.py:298-379); K(rho) u = F by a sparse
+    direct solve.  Returns (rho, compliance history, u)."""
+    nodes, conn = np.asarray(nodes, dtype=float), np.asarray(conn)
+    n_dof = 3 * len(nodes)
+    free = free_dofs(n_dof, fixed)
+    ke = hex8_element_stiffness(nodes[conn], D)
+    F_ext = np.asarray(F_ext, dtype=float)
+    rho = np.full(len(conn), float(volume_fraction))
+    H = None
+    if filter_radius is not None and filter_radius > 0:
+        H = build_filter_weights(nodes[conn].mean(axis=1), filter_radius)
+    hist, u = [], None
+    for _ in range(n_iter):
+        s = simp_scale(rho, p, rho_min)
+        Kff = reduce_free(structural_csr(ke * s[:, None, None], conn, n_dof), free).tocsc()
+        u = np.zeros(n_dof)
+        u[free] = spla.spsolve(Kff, F_ext[free])
+        hist.append(float(F_ext @ u))
+        dc = compliance_sensitivity_closed_form(ke, conn, u, rho, p, rho_min)
+        if H is not None:
+            dc = apply_sensitivity_filter(H, rho, dc)
+        new = oc_update(rho, dc, volume_fraction, move=move, rho_min_bound=rho_min)
+        change = float(np.max(np.abs(new - rho)))
+        rho = new
+        if change < tol:
+            break
+    return rho, hist, u
 
 
 # ----------------------------------------------------------------------------- recovery

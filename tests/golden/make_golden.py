@@ -28,6 +28,9 @@ simp_6x3x3.npz         SIMP compliance: densities, forward solution, closed-form
 pod_small.npz          singular values of a 400x12 snapshot matrix from PodBasis.fit.
 recovery_20x4x4.npz    the cantilever_20x4x4 system at its SuperLU displacement: FESystem.stress /
                        strain / von_mises at the nodes and per element, and reactions.
+topopt_8x4x4.npz       SIMP on an 8x4x4 cantilever: build_filter_weights, apply_sensitivity_filter,
+                       oc_update on seeded inputs, and 12 iterations of
+                       topology_optimize_compliance (final densities, compliance history, u).
 """
 from __future__ import annotations
 
@@ -221,6 +224,43 @@ def recovery_20x4x4():
                 reactions=np.asarray(fs.reactions(U)))
 
 
+def topopt_8x4x4():
+    """The reference's SIMP loop on a small hex8 cantilever (2.0 x 1.0 x 1.0, 8x4x4, E = 1,
+    nu = 0.3, x = 0 clamped, unit -z load at the tip node nearest (2, 0.5, 0)): filter weights,
+    one filtered sensitivity, one OC update on seeded inputs, and topology_optimize_compliance
+    (vf 0.4, p 3, rho_min 1e-2, move 0.2, filter radius 0.375, 12 iterations)."""
+    from fea_engine.mesh import box_mesh
+    from fea_engine.elements.solids import Hex8Solid3D
+    from fea_engine.material import Material, D_solid3d
+    from fea_engine.solver import FESystem
+    from fea_engine import topopt
+
+    mesh = box_mesh(2.0, 1.0, 1.0, 8, 4, 4)
+    fs = FESystem(mesh, Hex8Solid3D())
+    D = D_solid3d(Material(E=1.0, nu=0.3))
+    fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+    tip = mesh.nodes_on_plane(0, 2.0)
+    node = int(tip[np.argmin(np.linalg.norm(mesh.nodes[tip] - np.array([2.0, 0.5, 0.0]), axis=1))])
+    F = np.zeros(fs.n_dof)
+    F[3 * node + 2] = -1.0
+    conn = np.asarray(mesh.elements)
+    centroids = mesh.nodes[conn].mean(axis=1)
+    radius = 0.375
+    H = topopt.build_filter_weights(centroids, radius)
+    rng = np.random.default_rng(9)
+    rho_s = rng.uniform(0.05, 1.0, len(conn))
+    dc_s = -rng.uniform(0.1, 5.0, len(conn))
+    dc_s[::17] = rng.uniform(0.0, 1e-3, dc_s[::17].shape)        # a few non-negative entries
+    dc_filtered = topopt.apply_sensitivity_filter(H, rho_s, dc_s)
+    rho_oc = topopt.oc_update(rho_s, dc_s, 0.4, move=0.2, rho_min_bound=1e-2)
+    res = topopt.topology_optimize_compliance(fs, D, F, 0.4, p=3.0, rho_min=1e-2, move=0.2, n_iter=12,
+                                             filter_radius=radius, tol=1e-3)
+    return dict(nodes=np.asarray(mesh.nodes), elements=conn.astype(np.int64), D=D, F=F,
+                fixed=np.asarray(fs.fixed_dofs_array), radius=np.float64(radius), H=H, rho_s=rho_s, dc_s=dc_s,
+                dc_filtered=dc_filtered, rho_oc=rho_oc, rho_final=res["rho"],
+                compliance_history=np.asarray(res["compliance_history"]), u_final=res["u_final"])
+
+
 def pod_small():
     from rom_engine.pod import PodBasis
     rng = np.random.default_rng(3)
@@ -239,7 +279,8 @@ def main():
     _import_reference(args.reference)
     for name, fn in [("cantilever_20x4x4", cantilever_20x4x4), ("pattern_4x3x2", pattern_4x3x2),
                      ("ke_distorted", ke_distorted), ("facets", facets), ("simp_6x3x3", simp_6x3x3),
-                     ("pod_small", pod_small), ("recovery_20x4x4", recovery_20x4x4)]:
+                     ("pod_small", pod_small), ("recovery_20x4x4", recovery_20x4x4),
+                     ("topopt_8x4x4", topopt_8x4x4)]:
         if args.only and name not in args.only:
             continue
         data = fn()

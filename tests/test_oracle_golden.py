@@ -120,3 +120,18 @@ def test_recovery_matches_reference(golden):
     assert _relnorm(R, g["reactions"]) < 1e-9
     # the reactions balance the applied load (z: the -1e6 Pa traction on the 0.16 m^2 tip face)
     assert abs(R[2::3].sum() - 1.6e5) < 1e-6 * 1.6e5
+
+
+def test_simp_loop_matches_reference(golden):
+    g = golden("topopt_8x4x4")
+    X, el = g["nodes"], g["elements"]
+    H = O.build_filter_weights(X[el].mean(axis=1), float(g["radius"]))
+    assert np.array_equal(H, g["H"])
+    assert _relnorm(O.apply_sensitivity_filter(H, g["rho_s"], g["dc_s"]), g["dc_filtered"]) < 1e-14
+    assert np.array_equal(O.oc_update(g["rho_s"], g["dc_s"], 0.4, move=0.2, rho_min_bound=1e-2), g["rho_oc"])
+    rho, hist, u = O.topology_optimize_compliance(X, el, g["D"], g["fixed"], g["F"], 0.4, p=3.0, rho_min=1e-2,
+                                                  move=0.2, n_iter=12, filter_radius=float(g["radius"]), tol=1e-3)
+    assert len(hist) == len(g["compliance_history"])
+    assert np.max(np.abs(np.array(hist) - g["compliance_history"]) / g["compliance_history"]) < 1e-9
+    assert np.max(np.abs(rho - g["rho_final"])) < 1e-8
+    assert _relnorm(u, g["u_final"]) < 1e-8

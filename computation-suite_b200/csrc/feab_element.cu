@@ -22,6 +22,12 @@ __device__ __forceinline__ void pair_of(int pr, int& a, int& b) {
 // w*detJ into shared memory.  Phase 2: thread per (element, pair) contracts
 // K_ab[i][j] = sum_q wdet * sum_{s,t} B_a[s][i] D[s][t] B_b[t][j], using the 3 non-zeros
 // per column of B (row pattern of elements/solids.py:150-162).
+// BBAR (Hex8SolidBbar, elements/solids.py:225-257): B is replaced by the mean-dilatation
+// B-bar = B - (m m^T / 3) B + (m m^T / 3) B-averaged, B-averaged = sum_q B detJ w / sum_q detJ w
+// (m = [1 1 1 0 0 0]); in the three normal-strain rows the column of node k, component j becomes
+// delta_ij g_k,i - g_k,j / 3 + gbar_k,j / 3 with gbar_k the volume-averaged gradient, so the
+// columns have 5 non-zeros and phase 2 contracts the full 6 x 3 column blocks.
+template <bool BBAR>
 __global__ void __launch_bounds__(kKeThreads) k_hex8_ke(const double* __restrict__ coords, const int32_t* __restrict__ conn,
                                                         int64_t n_elem, Mat6 D, const double* __restrict__ scale,
                                                         double thickness, double* __restrict__ ke, int layout,
@@ -29,6 +35,7 @@ __global__ void __launch_bounds__(kKeThreads) k_hex8_ke(const double* __restrict
   __shared__ double sX[kKeElems][8][3];
   __shared__ double sG[kKeElems][8][8][3];
   __shared__ double sW[kKeElems][8];
+  __shared__ double sGbar[BBAR ? kKeElems : 1][8][3];
   const int t = threadIdx.x;
   const int64_t e0 = (int64_t)blockIdx.x * kKeElems;
   {
@@ -66,6 +73,25 @@ __global__ void __launch_bounds__(kKeThreads) k_hex8_ke(const double* __restrict
     }
   }
   __syncthreads();
+  if (BBAR) {
+    // thread (element, k): the volume-averaged gradient of node k (Gauss points in rule order)
+    const int el = t >> 3, k = t & 7;
+    if (e0 + el < n_elem) {
+      double gx = 0.0, gy = 0.0, gz = 0.0, vol = 0.0;
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        const double w = sW[el][q];
+        gx += sG[el][q][k][0] * w;
+        gy += sG[el][q][k][1] * w;
+        gz += sG[el][q][k][2] * w;
+        vol += w;
+      }
+      sGbar[el][k][0] = gx / vol;
+      sGbar[el][k][1] = gy / vol;
+      sGbar[el][k][2] = gz / vol;
+    }
+    __syncthreads();
+  }
   for (int task = t; task < kKeElems * 36; task += kKeThreads) {
     const int el = task / 36, pr = task % 36;
     const int64_t e = e0 + el;
@@ -73,6 +99,55 @@ __global__ void __launch_bounds__(kKeThreads) k_hex8_ke(const double* __restrict
     int a, b;
     pair_of(pr, a, b);
     double K[3][3] = {{0, 0, 0}, {0, 0, 0}, {0, 0, 0}};
+    if (BBAR) {
+      // B-bar column blocks Ba, Bb (6 x 3) at each Gauss point; K_ab += w Ba^T D Bb
+      const double (&ga)[3] = sGbar[el][a];
+      const double (&gb)[3] = sGbar[el][b];
+#pragma unroll 1
+      for (int q = 0; q < 8; ++q) {
+        const double w = sW[el][q];
+        double Ba[6][3], Bb[6][3];
+        auto column = [&](const double (&g)[3], const double (&gbar)[3], double (&B)[6][3]) {
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            const double vol = (gbar[j] - g[j]) / 3.0;
+#pragma unroll
+            for (int i = 0; i < 3; ++i) B[i][j] = (i == j ? g[i] : 0.0) + vol;
+          }
+          B[3][0] = g[1];
+          B[3][1] = g[0];
+          B[3][2] = 0.0;
+          B[4][0] = 0.0;
+          B[4][1] = g[2];
+          B[4][2] = g[1];
+          B[5][0] = g[2];
+          B[5][1] = 0.0;
+          B[5][2] = g[0];
+        };
+        const double gqa[3] = {sG[el][q][a][0], sG[el][q][a][1], sG[el][q][a][2]};
+        const double gqb[3] = {sG[el][q][b][0], sG[el][q][b][1], sG[el][q][b][2]};
+        column(gqa, ga, Ba);
+        column(gqb, gb, Bb);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          double DB[6];
+#pragma unroll
+          for (int s = 0; s < 6; ++s) {
+            double v = 0.0;
+#pragma unroll
+            for (int r = 0; r < 6; ++r) v += D.d[s * 6 + r] * Bb[r][j];
+            DB[s] = v;
+          }
+#pragma unroll
+          for (int i = 0; i < 3; ++i) {
+            double v = 0.0;
+#pragma unroll
+            for (int s = 0; s < 6; ++s) v += Ba[s][i] * DB[s];
+            K[i][j] += w * v;
+          }
+        }
+      }
+    } else
 #pragma unroll 2
     for (int q = 0; q < 8; ++q) {
       const double w = sW[el][q];
@@ -223,19 +298,37 @@ static bool load_mat6(const double* D_host, Mat6* out) {
   return true;
 }
 
-extern "C" int32_t feab_hex8_element_stiffness(const double* coords, const int32_t* conn, int64_t n_elem,
-                                               const double* D_host, const double* scale, double thickness,
-                                               double* ke_out, int32_t layout, feab_device_status* status,
-                                               cudaStream_t s) {
+static int32_t element_stiffness(bool bbar, const double* coords, const int32_t* conn, int64_t n_elem,
+                                 const double* D_host, const double* scale, double thickness, double* ke_out,
+                                 int32_t layout, feab_device_status* status, cudaStream_t s) {
   Mat6 D;
   if (!coords || !conn || !ke_out || n_elem < 0 || !load_mat6(D_host, &D)) return FEAB_BAD_ARG;
   if (layout != FEAB_HEX8_KE_PACKED && layout != FEAB_HEX8_KE_FULL) return FEAB_BAD_ARG;
   if (n_elem == 0) return FEAB_OK;
   const int64_t grid = (n_elem + kKeElems - 1) / kKeElems;
   count_launches(1);
-  k_hex8_ke<<<(unsigned)grid, kKeThreads, 0, s>>>(coords, conn, n_elem, D, scale, thickness, ke_out, layout, status);
+  if (bbar)
+    k_hex8_ke<true><<<(unsigned)grid, kKeThreads, 0, s>>>(coords, conn, n_elem, D, scale, thickness, ke_out, layout,
+                                                          status);
+  else
+    k_hex8_ke<false><<<(unsigned)grid, kKeThreads, 0, s>>>(coords, conn, n_elem, D, scale, thickness, ke_out, layout,
+                                                           status);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;
+}
+
+extern "C" int32_t feab_hex8_element_stiffness(const double* coords, const int32_t* conn, int64_t n_elem,
+                                               const double* D_host, const double* scale, double thickness,
+                                               double* ke_out, int32_t layout, feab_device_status* status,
+                                               cudaStream_t s) {
+  return element_stiffness(false, coords, conn, n_elem, D_host, scale, thickness, ke_out, layout, status, s);
+}
+
+extern "C" int32_t feab_hex8_bbar_element_stiffness(const double* coords, const int32_t* conn, int64_t n_elem,
+                                                    const double* D_host, const double* scale, double thickness,
+                                                    double* ke_out, int32_t layout, feab_device_status* status,
+                                                    cudaStream_t s) {
+  return element_stiffness(true, coords, conn, n_elem, D_host, scale, thickness, ke_out, layout, status, s);
 }
 
 extern "C" int32_t feab_hex8_apply(const double* ke_packed, const int32_t* conn, const int32_t* inc_ptr,

@@ -254,8 +254,9 @@ class DeviceMesh:
         return pat
 
     # ------------------------------------------------------------------ element matrices
-    def element_stiffness(self, D, scale=None, thickness=1.0, layout=L.KE_PACKED, status=None):
-        """Element stiffness matrices, (E, 324) packed upper node blocks or (E, 24, 24)."""
+    def element_stiffness(self, D, scale=None, thickness=1.0, layout=L.KE_PACKED, status=None, bbar=False):
+        """Element stiffness matrices, (E, 324) packed upper node blocks or (E, 24, 24); with
+        bbar=True those of Hex8SolidBbar (mean-dilatation B-bar)."""
         st = status or DeviceStatus(self.device)
         width = L.KE_PACKED if layout == L.KE_PACKED else L.KE_FULL
         ke = torch.empty((self.n_elem, width), dtype=torch.float64, device=self.device)
@@ -264,8 +265,9 @@ class DeviceMesh:
             sc = torch.as_tensor(scale, dtype=torch.float64).to(self.device).contiguous()
             if sc.shape != (self.n_elem,):
                 raise ValueError(f"scale must have shape ({self.n_elem},)")
-        rc = L.lib.feab_hex8_element_stiffness(L.dptr(self.coords), L.dptr(self.conn), self.n_elem, L.dmat(D),
-                                               L.dptr(sc), float(thickness), L.dptr(ke), width, st.ptr(), self.stream)
+        fn = L.lib.feab_hex8_bbar_element_stiffness if bbar else L.lib.feab_hex8_element_stiffness
+        rc = fn(L.dptr(self.coords), L.dptr(self.conn), self.n_elem, L.dmat(D), L.dptr(sc), float(thickness),
+                L.dptr(ke), width, st.ptr(), self.stream)
         L.raise_for(rc, "hex8 element stiffness")
         if status is None:
             st.check("hex8 element stiffness")

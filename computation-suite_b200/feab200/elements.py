@@ -1,4 +1,5 @@
-"""The hex8 solid element formulation (Hex8Solid3D, elements/solids.py:130-163).
+"""The hex8 solid element formulations: Hex8Solid3D (elements/solids.py:130-163) and the
+mean-dilatation Hex8SolidBbar (elements/solids.py:225-270).
 
 The element matrices themselves are computed on the GPU (libfeab200); this class carries the
 formulation's identity and constants, and host-side shape functions for load integration."""
@@ -32,9 +33,33 @@ class Hex8Solid3D:
         coords = np.asarray(elem_coords, dtype=float).reshape(8, 3)
         dm = DeviceMesh(coords, np.arange(8)[None, :], device=device)
         from . import _lib as L
-        return dm.element_stiffness(D, thickness=thickness, layout=L.KE_FULL)[0].cpu().numpy()
+        return dm.element_stiffness(D, thickness=thickness, layout=L.KE_FULL, bbar=is_bbar(self))[0].cpu().numpy()
+
+    def full_stiffness(self, elem_coords, D, thickness=1.0):
+        return self.stiffness(elem_coords, D, thickness)
+
+
+class Hex8SolidBbar(Hex8Solid3D):
+    """Hex8 with the mean-dilatation B-bar: at each of the 8 Gauss points the volumetric part of
+    B is replaced by its volume average (elements/solids.py:225-257), which relieves volumetric
+    locking as nu -> 0.5.  Its element matrices come from feab_hex8_bbar_element_stiffness."""
+
+    def stiffness(self, elem_coords, D, thickness=1.0, gauss_order=None, device=None):
+        """B-bar is only defined at the full 8-point rule; gauss_order is ignored, as in the
+        reference (elements/solids.py:250-262)."""
+        return super().stiffness(elem_coords, D, thickness=thickness, gauss_order=None, device=device)
+
+    def reduced_stiffness(self, elem_coords, D, thickness=1.0):
+        raise NotImplementedError(
+            "Hex8SolidBbar has no reduced-integration variant -- B-bar's mean-dilatation correction is only "
+            "meaningful at the full 8-point rule. Use Hex8Solid3D for a reduced-integration Hex8.")
 
 
 def is_hex8(formulation):
-    """Accept this package's Hex8Solid3D or the reference's class of the same name."""
-    return type(formulation).__name__ == "Hex8Solid3D" and getattr(formulation, "n_nodes", 8) == 8
+    """Accept this package's Hex8Solid3D / Hex8SolidBbar or the reference's classes of those names."""
+    return (type(formulation).__name__ in ("Hex8Solid3D", "Hex8SolidBbar")
+            and getattr(formulation, "n_nodes", 8) == 8)
+
+
+def is_bbar(formulation):
+    return type(formulation).__name__ == "Hex8SolidBbar"

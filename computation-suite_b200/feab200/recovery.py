@@ -52,6 +52,10 @@ def _check_at(at):
 
 
 def _recover(system, U, D, kind, at, von_mises=False):
+    if type(system.elem).__name__ != "Hex8Solid3D":
+        # coefficients.check_supported (coefficients.py:107-111): recovery covers Hex8Solid3D only
+        raise NotImplementedError(f"{kind} recovery is not available for {type(system.elem).__name__}; "
+                                  f"supported: Hex8Solid3D.")
     U = _check_vector(system, U)
     Dm = _resolve_D(system, D) if kind == "stress" else None
     out = system.device_mesh.recover(U, Dm, nodal=at == "nodes", elements=at == "elements", von_mises=von_mises)

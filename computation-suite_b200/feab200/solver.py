@@ -26,7 +26,7 @@ import torch
 
 from . import _lib as L
 from .device import DeviceMesh, DeviceStatus, cuda_device, pcg_solve
-from .elements import is_hex8
+from .elements import is_bbar, is_hex8
 from .facet_loads import facet_load_shares_batch
 from .fields import FEField
 
@@ -39,7 +39,8 @@ class FESystem:
             raise NotImplementedError("FESystem: multi-block meshes are not supported on the hex8 GPU path")
         if not is_hex8(elem_formulation):
             raise NotImplementedError(
-                f"FESystem: only Hex8Solid3D is implemented on the GPU path, got {type(elem_formulation).__name__}")
+                f"FESystem: only Hex8Solid3D and Hex8SolidBbar are implemented on the GPU path, got "
+                f"{type(elem_formulation).__name__}")
         nodes = np.asarray(mesh.nodes, dtype=float)
         if nodes.ndim != 2 or nodes.shape[1] != 3:
             raise ValueError("FESystem: a hex8 solid mesh needs 3-D node coordinates")
@@ -171,7 +172,7 @@ class FESystem:
             warnings.warn("assemble_stiffness: K was already assembled, so it is being REPLACED. Pass "
                           "accumulate=True to add to the existing matrix instead.", UserWarning, stacklevel=2)
             self._warned_reassembly.add("K")
-        ke = self.device_mesh.element_stiffness(D, thickness=thickness)
+        ke = self.device_mesh.element_stiffness(D, thickness=thickness, bbar=is_bbar(self.elem))
         if accumulate and self._ke is not None:
             self._ke = self._ke + ke
         else:

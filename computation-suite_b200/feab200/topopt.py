@@ -19,6 +19,7 @@ import torch
 
 from . import _lib as L
 from .device import DeviceMesh, DeviceStatus, cuda_device, pcg_solve
+from .elements import is_bbar
 
 
 def simp_scale(rho, p=3.0, rho_min=1e-3):
@@ -69,6 +70,11 @@ def unit_stiffness_stack(fesystem, D, gauss_order=None):
     """(ke_unit, connectivity) at rho = 1 (topopt.py:96-105)."""
     if gauss_order not in (None, 2):
         raise NotImplementedError("unit_stiffness_stack: only the full 2x2x2 rule is implemented")
+    if is_bbar(fesystem.elem):
+        # the reference builds the stack with MeshTransformation, which refuses elements that
+        # override Element.stiffness (mesh_transform.py:155-170)
+        raise ValueError("unit_stiffness_stack: Hex8SolidBbar overrides the element stiffness; the SIMP "
+                         "path supports Hex8Solid3D")
     return UnitStiffnessStack(fesystem.device_mesh, D), np.asarray(fesystem.mesh.elements)
 
 
@@ -350,6 +356,9 @@ def topology_optimize_compliance(fesystem, D, F_ext, volume_fraction, p=3.0, rho
     if sensitivity not in ("closed_form", "adjoint"):
         raise ValueError(f"topology_optimize_compliance: unknown sensitivity={sensitivity!r} "
                          f"-- expected 'closed_form' or 'adjoint'.")
+    if is_bbar(fesystem.elem):
+        raise ValueError("topology_optimize_compliance: Hex8SolidBbar overrides the element stiffness; the SIMP "
+                         "path supports Hex8Solid3D (as the reference's MeshTransformation does)")
     dm = fesystem.device_mesh
     dev = dm.device
     free = fesystem.free_dofs

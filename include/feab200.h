@@ -187,6 +187,14 @@ int32_t feab_hex8_element_stiffness(const double* coords, const int32_t* conn, i
                                     double* ke_out, int32_t layout, feab_device_status* status,
                                     cudaStream_t stream);
 
+/* The same for Hex8SolidBbar (elements/solids.py:225-257): B replaced by the mean-dilatation
+ * B-bar = B - (m m^T / 3) B + (m m^T / 3) sum_q B detJ w / sum_q detJ w, m = [1 1 1 0 0 0], at
+ * the same 8 Gauss points (signed detJ in both sums). */
+int32_t feab_hex8_bbar_element_stiffness(const double* coords, const int32_t* conn, int64_t n_elem,
+                                         const double* D_host, const double* scale, double thickness,
+                                         double* ke_out, int32_t layout, feab_device_status* status,
+                                         cudaStream_t stream);
+
 /* ---------------------------------------------------------------- assembly
  * Deterministic gather assembly of the reduced CSR values from packed element
  * matrices: each entry is summed over its elements in ascending element order.

@@ -17,7 +17,7 @@ import scipy.sparse.linalg as spla
 
 __all__ = [
     "gauss_legendre", "box_mesh", "perturb_interior", "D_solid3d", "hex8_shape_and_derivs",
-    "hex8_element_stiffness", "global_dofs", "structural_csr", "reduce_free", "fixed_dofs_on_plane",
+    "hex8_element_stiffness", "hex8_bbar_element_stiffness", "global_dofs", "structural_csr", "reduce_free", "fixed_dofs_on_plane",
     "free_dofs", "quad4_shape_and_derivs", "HEX8_FACES", "facet_load_shares", "facet_mass",
     "jacobi_inverse_diagonal", "preconditioned_cg", "simp_scale", "simp_scale_grad",
     "compliance_sensitivity_closed_form", "pod_singular_values", "element_strain_energy_density",
@@ -158,6 +158,24 @@ def hex8_element_stiffness(coords, D, thickness=1.0):
     for w, detJ, dN_g in _gauss_geometry(coords):
         B = _b_matrices(dN_g)
         ke += np.matmul(np.transpose(B, (0, 2, 1)), np.matmul(D, B)) * (detJ * w * thickness)[:, None, None]
+    return ke
+
+
+def hex8_bbar_element_stiffness(coords, D, thickness=1.0):
+    """Element stiffness of Hex8SolidBbar (fea_engine/src/fea_engine/elements/solids.py:228-257):
+    at each Gauss point B-bar = B - P B + P Bavg, P = m m^T / 3 (m = [1 1 1 0 0 0]),
+    Bavg = sum_q B detJ w / sum_q detJ w (signed detJ); ke = sum_q B-bar^T D B-bar detJ w."""
+    coords = np.asarray(coords, dtype=float)
+    D = np.asarray(D, dtype=float)
+    m = np.array([1.0, 1.0, 1.0, 0.0, 0.0, 0.0])
+    P = np.outer(m, m) / 3.0
+    geo = [(w, detJ, _b_matrices(dN_g)) for w, detJ, dN_g in _gauss_geometry(coords)]
+    vol = sum(detJ * w for w, detJ, _ in geo)
+    Bavg = sum(np.matmul(P, B) * (detJ * w)[:, None, None] for w, detJ, B in geo) / vol[:, None, None]
+    ke = np.zeros((coords.shape[0], 24, 24))
+    for w, detJ, B in geo:
+        Bb = B - np.matmul(P, B) + Bavg
+        ke += np.matmul(np.transpose(Bb, (0, 2, 1)), np.matmul(D, Bb)) * (detJ * w * thickness)[:, None, None]
     return ke
 
 

@@ -28,6 +28,8 @@ simp_6x3x3.npz         SIMP compliance: densities, forward solution, closed-form
 pod_small.npz          singular values of a 400x12 snapshot matrix from PodBasis.fit.
 recovery_20x4x4.npz    the cantilever_20x4x4 system at its SuperLU displacement: FESystem.stress /
                        strain / von_mises at the nodes and per element, and reactions.
+bbar_hex8.npz          Hex8SolidBbar element stiffness of distorted hexes (nu 0.3, 0.4999) and the
+                       near-incompressible cantilever deflection with Hex8SolidBbar and Hex8Solid3D.
 topopt_8x4x4.npz       SIMP on an 8x4x4 cantilever: build_filter_weights, apply_sensitivity_filter,
                        oc_update on seeded inputs, and 12 iterations of
                        topology_optimize_compliance (final densities, compliance history, u).
@@ -261,6 +263,39 @@ def topopt_8x4x4():
                 compliance_history=np.asarray(res["compliance_history"]), u_final=res["u_final"])
 
 
+def bbar_hex8():
+    """Hex8SolidBbar: element stiffness of 6 distorted hexes at nu = 0.3 and 0.4999, and the tip
+    deflection of the reference's locking benchmark (fea_engine/tests/test_hex8_bbar.py:122-143:
+    1.0 x 0.05 x 0.05 cantilever, 20x4x4, -1000 N on the tip face) with Hex8SolidBbar and
+    Hex8Solid3D at nu = 0.4999, solved by FESystem.solve_static."""
+    from fea_engine.elements.solids import Hex8Solid3D, Hex8SolidBbar
+    from fea_engine.material import Material, D_solid3d
+    from fea_engine.mesh import box_mesh
+    from fea_engine.solver import FESystem
+
+    rng = np.random.default_rng(17)
+    cube = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    coords = np.stack([cube * rng.uniform(0.3, 2.0, 3) + 0.12 * rng.standard_normal((8, 3)) for _ in range(6)])
+    out = dict(coords=coords)
+    for tag, nu in (("03", 0.3), ("04999", 0.4999)):
+        D = D_solid3d(Material(E=2.1e11, nu=nu))
+        out["D_" + tag] = D
+        out["ke_" + tag] = np.stack([Hex8SolidBbar().stiffness(c, D) for c in coords])
+    mesh = box_mesh(1.0, 0.05, 0.05, 20, 4, 4)
+    D = out["D_04999"]
+    tip = mesh.nodes_on_plane(0, 1.0)
+    for name, cls in (("bbar", Hex8SolidBbar), ("plain", Hex8Solid3D)):
+        fs = FESystem(mesh, cls())
+        fs.assemble_stiffness(D)
+        fs.add_nodal_force(tip, dof_index=2, total_force=-1000.0)
+        fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+        out["U_" + name] = np.asarray(fs.solve_static())
+    out["nodes"] = np.asarray(mesh.nodes)
+    out["elements"] = np.asarray(mesh.elements, dtype=np.int64)
+    out["F"] = np.asarray(fs.F)
+    return out
+
+
 def pod_small():
     from rom_engine.pod import PodBasis
     rng = np.random.default_rng(3)
@@ -280,7 +315,7 @@ def main():
     for name, fn in [("cantilever_20x4x4", cantilever_20x4x4), ("pattern_4x3x2", pattern_4x3x2),
                      ("ke_distorted", ke_distorted), ("facets", facets), ("simp_6x3x3", simp_6x3x3),
                      ("pod_small", pod_small), ("recovery_20x4x4", recovery_20x4x4),
-                     ("topopt_8x4x4", topopt_8x4x4)]:
+                     ("topopt_8x4x4", topopt_8x4x4), ("bbar_hex8", bbar_hex8)]:
         if args.only and name not in args.only:
             continue
         data = fn()

@@ -135,3 +135,10 @@ def test_simp_loop_matches_reference(golden):
     assert np.max(np.abs(np.array(hist) - g["compliance_history"]) / g["compliance_history"]) < 1e-9
     assert np.max(np.abs(rho - g["rho_final"])) < 1e-8
     assert _relnorm(u, g["u_final"]) < 1e-8
+
+
+def test_bbar_element_stiffness_matches_reference(golden):
+    g = golden("bbar_hex8")
+    for tag in ("03", "04999"):
+        ke = O.hex8_bbar_element_stiffness(g["coords"], g["D_" + tag])
+        assert _relnorm(ke, g["ke_" + tag]) < 1e-14

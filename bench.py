@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery",
-                                           "simp_oc"],
+                                           "simp_oc", "elements", "modal"],
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
@@ -770,6 +770,101 @@ def workload_simp_oc(args):
                                                        "24x8x8, 3 iterations"}}
 
 
+def workload_elements(args):
+    """The element-matrix kernels alone on the 128x32x32 cantilever (packed layout, L2 flushed
+    before each launch): Hex8Solid3D and Hex8SolidBbar.  Work per element, counted from the
+    contractions: plain 8 x 36 x (54 + 27) FMA (D B for the 3 non-zeros of each B column, then
+    B^T (D B)); B-bar 8 x 36 x 162 FMA (full 6 x 3 column blocks), plus the Jacobian per Gauss
+    point; HBM: 324 doubles written per element."""
+    import torch
+    from feab200.device import DeviceMesh
+    c = build_workload(tuple(args.shape))
+    dm = DeviceMesh(c.mesh.nodes, c.mesh.elements)
+    E = dm.n_elem
+    flush = L2Flush(dm.device)
+    out = {}
+    for name, bbar, fma in (("plain", False, 8 * 36 * 81), ("bbar", True, 8 * 36 * 162)):
+        dm.element_stiffness(c.D, bbar=bbar)
+        times = []
+        for _ in range(max(3, args.steps)):
+            flush()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            dm.element_stiffness(c.D, bbar=bbar, status=_NO_CHECK)
+            b.record()
+            torch.cuda.synchronize()
+            times.append(a.elapsed_time(b) * 1e-3)
+        t = statistics.mean(times)
+        out[name] = {"us": round(t * 1e6, 1), "fp64_tflops": round(2 * fma * E / t / 1e12, 2),
+                     "write_gbs": round(324 * 8 * E / t / 1e9, 1)}
+    return {"metric": f"hex8 element stiffness kernel time (Hex8Solid3D and Hex8SolidBbar), "
+                      f"{'x'.join(map(str, args.shape))}, packed layout",
+            "value": out["plain"]["us"], "unit": "us", "n_elements": E, "kernels": out,
+            "timing": "CUDA events around each launch, L2 flushed before each"}
+
+
+def workload_modal(args):
+    """The 6 lowest natural frequencies of the cantilever (2.0 x 0.4 x 0.4 m, steel, x = 0 clamped)
+    meshed 64x16x16 (52,224 free DOFs): consistent mass + FESystem.solve_modal (GPU block
+    subspace iteration with block-PCG inner solves).  The oracle (the reference's shift-invert
+    eigsh with a sparse LU) runs on the 32x8x8 mesh, where the GPU solve is repeated for the
+    frequency comparison."""
+    import torch
+    import feab200
+    import oracle as O
+
+    def system(shape):
+        nodes, el = O.box_mesh(2.0, 0.4, 0.4, *shape)
+        mesh = feab200.Mesh(nodes=nodes, elements=el)
+        fs = feab200.FESystem(mesh, feab200.Hex8Solid3D(), sparse=True)
+        fs.assemble_stiffness(O.D_solid3d(210e9, 0.3))
+        fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+        fs.assemble_mass(7850.0 * np.eye(3))
+        return fs, nodes, el
+
+    fs, _, _ = system((64, 16, 16))
+    fs.solve_modal(6)                                                   # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    f, _ = fs.solve_modal(6)
+    torch.cuda.synchronize()
+    gpu_ms = (time.perf_counter() - t0) * 1e3
+    iters = fs.last_modal_iterations
+    fs_s, nodes, el = system((32, 8, 8))
+    f_s, _ = fs_s.solve_modal(6)
+    free = fs_s.free_dofs
+    Kff = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(nodes[el], O.D_solid3d(210e9, 0.3)), el,
+                                         3 * len(nodes)), free)
+    Mff = O.reduce_free(O.structural_csr(O.hex8_element_mass(nodes[el], 7850.0 * np.eye(3)), el, 3 * len(nodes)), free)
+    t0 = time.perf_counter()
+    f_ref, _ = O.modal(Kff, Mff, 6)
+    cpu_ms = (time.perf_counter() - t0) * 1e3
+    return {"metric": "hex8 modal solve time (6 lowest modes, consistent mass), 64x16x16 cantilever",
+            "value": round(gpu_ms, 1), "unit": "ms", "free_dofs": int(fs.reduced_operator(want32=False).n),
+            "subspace_iterations": iters, "freq_hz": [float(v) for v in f],
+            "rel_err_vs_eigsh_32x8x8": float(np.max(np.abs(f_s - f_ref) / f_ref)),
+            "cpu_baseline": {"value": round(cpu_ms, 1), "unit": "ms", "cores": os.cpu_count(), "kind": "port",
+                             "sample": "oracle shift-invert eigsh (SciPy, sparse LU) on the 32x8x8 mesh; the "
+                                       "64x16x16 mesh takes about a minute on 8 cores"}}
+
+
+class _NoCheck:
+    """A device status that is never read back, so a timed element-matrix launch has no sync."""
+
+    def __init__(self):
+        self.t = None
+
+    def ptr(self):
+        import torch
+        if self.t is None:
+            self.t = torch.zeros(2, dtype=torch.int64, device="cuda")
+        from feab200 import _lib as L
+        return L.dptr(self.t)
+
+
+_NO_CHECK = _NoCheck()
+
+
 # ----------------------------------------------------------------------------- main
 def main():
     args = parse()
@@ -779,7 +874,7 @@ def main():
     if args.workload != "cantilever" and args.impl == "ours":
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
               "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery,
-              "simp_oc": workload_simp_oc}[args.workload]
+              "simp_oc": workload_simp_oc, "elements": workload_elements, "modal": workload_modal}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})

@@ -192,6 +192,82 @@ __global__ void __launch_bounds__(kKeThreads) k_hex8_ke(const double* __restrict
   }
 }
 
+// Consistent mass (Element.mass, elements/base.py:711-731): me = sum_q Nm^T R Nm |detJ| w t, so the
+// (a, b) node block is m_ab R t with m_ab = sum_q N_a N_b |detJ| w and R the 3x3 density matrix.
+// Thread (element, q) forms |detJ_q| into shared memory; thread (element, pair a <= b) sums m_ab
+// over the Gauss points in rule order and writes the block (packed) or both blocks (full).
+__global__ void __launch_bounds__(kKeThreads) k_hex8_mass(const double* __restrict__ coords,
+                                                          const int32_t* __restrict__ conn, int64_t n_elem, Mat6 R,
+                                                          const double* __restrict__ scale, double thickness,
+                                                          double* __restrict__ me, int layout,
+                                                          feab_device_status* st) {
+  __shared__ double sX[kKeElems][8][3];
+  __shared__ double sDet[kKeElems][8];
+  const int t = threadIdx.x;
+  const int64_t e0 = (int64_t)blockIdx.x * kKeElems;
+  {
+    const int el = t >> 3, k = t & 7;
+    const int64_t e = e0 + el;
+    if (e < n_elem) {
+      const int64_t n = conn[e * 8 + k];
+      sX[el][k][0] = coords[n * 3 + 0];
+      sX[el][k][1] = coords[n * 3 + 1];
+      sX[el][k][2] = coords[n * 3 + 2];
+    }
+  }
+  __syncthreads();
+  {
+    const int el = t >> 3, q = t & 7;
+    const int64_t e = e0 + el;
+    if (e < n_elem) {
+      double X[8][3];
+#pragma unroll
+      for (int k = 0; k < 8; ++k)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) X[k][j] = sX[el][k][j];
+      double xi, eta, zeta, inv[3][3];
+      gauss_point(q, xi, eta, zeta);
+      const double det = jacobian_inverse(X, xi, eta, zeta, inv);
+      if (!(fabs(det) >= 1e-300)) set_status(reinterpret_cast<int*>(st), FEAB_DEGENERATE_ELEMENT, e);
+      sDet[el][q] = fabs(det);  // w = 1 for the 2-point rule
+    }
+  }
+  __syncthreads();
+  for (int task = t; task < kKeElems * 36; task += kKeThreads) {
+    const int el = task / 36, pr = task % 36;
+    const int64_t e = e0 + el;
+    if (e >= n_elem) break;
+    int a, b;
+    pair_of(pr, a, b);
+    double m = 0.0;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      double xi, eta, zeta;
+      gauss_point(q, xi, eta, zeta);
+      const double Na = 0.125 * (1.0 + xi * xi_sign(a)) * (1.0 + eta * eta_sign(a)) * (1.0 + zeta * zeta_sign(a));
+      const double Nb = 0.125 * (1.0 + xi * xi_sign(b)) * (1.0 + eta * eta_sign(b)) * (1.0 + zeta * zeta_sign(b));
+      m += Na * Nb * sDet[el][q];
+    }
+    const double f = m * thickness * (scale ? scale[e] : 1.0);
+    if (layout == FEAB_HEX8_KE_PACKED) {
+      double* o = me + (e * 36 + pr) * 9;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) o[i * 3 + j] = R.d[i * 3 + j] * f;
+    } else {
+      double* o = me + e * 576;
+#pragma unroll
+      for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+          o[(3 * a + i) * 24 + 3 * b + j] = R.d[i * 3 + j] * f;
+          if (a != b) o[(3 * b + j) * 24 + 3 * a + i] = R.d[i * 3 + j] * f;
+        }
+    }
+  }
+}
+
 // y[3a+i] = sum over elements e of a, local nodes lb, dofs j: K_e(la,lb)[i][j] v[3 b + j].
 // One warp per node; 72 (lb, i, j) terms per element spread over the lanes.
 __global__ void k_hex8_apply(const double* __restrict__ ke, const int32_t* __restrict__ conn,
@@ -329,6 +405,24 @@ extern "C" int32_t feab_hex8_bbar_element_stiffness(const double* coords, const 
                                                     double* ke_out, int32_t layout, feab_device_status* status,
                                                     cudaStream_t s) {
   return element_stiffness(true, coords, conn, n_elem, D_host, scale, thickness, ke_out, layout, status, s);
+}
+
+extern "C" int32_t feab_hex8_element_mass(const double* coords, const int32_t* conn, int64_t n_elem,
+                                          const double* R_host, const double* scale, double thickness, double* me_out,
+                                          int32_t layout, feab_device_status* status, cudaStream_t s) {
+  if (!coords || !conn || !me_out || !R_host || n_elem < 0) return FEAB_BAD_ARG;
+  if (layout != FEAB_HEX8_KE_PACKED && layout != FEAB_HEX8_KE_FULL) return FEAB_BAD_ARG;
+  Mat6 R;  // the 3x3 density matrix in the first 9 entries
+  for (int i = 0; i < 36; ++i) R.d[i] = i < 9 ? R_host[i] : 0.0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < i; ++j)
+      if (R.d[i * 3 + j] != R.d[j * 3 + i]) return FEAB_BAD_ARG;  // the packed blocks assume R = R^T
+  if (n_elem == 0) return FEAB_OK;
+  const int64_t grid = (n_elem + kKeElems - 1) / kKeElems;
+  count_launches(1);
+  k_hex8_mass<<<(unsigned)grid, kKeThreads, 0, s>>>(coords, conn, n_elem, R, scale, thickness, me_out, layout, status);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
 }
 
 extern "C" int32_t feab_hex8_apply(const double* ke_packed, const int32_t* conn, const int32_t* inc_ptr,

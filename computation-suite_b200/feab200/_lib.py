@@ -86,6 +86,7 @@ SIGNATURES = {
     "feab_csr_pattern": (_I32, [_P, _P, _I32, _P, _I32, _P, _P, _P, _P, _SZ, C.POINTER(_I64), C.POINTER(_I32), _P]),
     "feab_hex8_element_stiffness": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _P, _I32, _P, _P]),
     "feab_hex8_bbar_element_stiffness": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _P, _I32, _P, _P]),
+    "feab_hex8_element_mass": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _P, _I32, _P, _P]),
     "feab_assemble_csr": (_I32, [_P, _P, _P, _P, _P, _P, _I32, _I32, _P, _P, _P, _P, _P, _P, _P, _P]),
     "feab_hex8_apply": (_I32, [_P, _P, _P, _P, _I32, _P, _P, _P]),
     "feab_pcg_workspace_bytes": (_SZ, [_I32, _I32]),

@@ -273,6 +273,28 @@ class DeviceMesh:
             st.check("hex8 element stiffness")
         return ke if width == L.KE_PACKED else ke.view(self.n_elem, 24, 24)
 
+    def element_mass(self, R, scale=None, thickness=1.0, layout=L.KE_PACKED, status=None):
+        """Consistent element mass matrices for the 3x3 density matrix R (e.g. rho * I), in the
+        layouts of element_stiffness (Element.mass, elements/base.py:711-731)."""
+        R = np.asarray(R, dtype=float)
+        if R.shape != (3, 3):
+            raise ValueError(f"the density matrix of a hex8 solid must be 3x3, got shape {R.shape}")
+        if not np.array_equal(R, R.T):
+            raise ValueError("the density matrix must be symmetric")
+        st = status or DeviceStatus(self.device)
+        width = L.KE_PACKED if layout == L.KE_PACKED else L.KE_FULL
+        me = torch.empty((self.n_elem, width), dtype=torch.float64, device=self.device)
+        sc = None
+        if scale is not None:
+            sc = torch.as_tensor(scale, dtype=torch.float64).to(self.device).contiguous()
+        Rh = (C.c_double * 9)(*R.reshape(9).tolist())
+        rc = L.lib.feab_hex8_element_mass(L.dptr(self.coords), L.dptr(self.conn), self.n_elem, Rh, L.dptr(sc),
+                                          float(thickness), L.dptr(me), width, st.ptr(), self.stream)
+        L.raise_for(rc, "hex8 element mass")
+        if status is None:
+            st.check("hex8 element mass")
+        return me if width == L.KE_PACKED else me.view(self.n_elem, 24, 24)
+
     def assemble(self, ke_packed, pattern: Pattern, want32=True, status=None) -> ReducedOperator:
         topo = self.topology()
         dev = self.device

@@ -1,0 +1,81 @@
+"""Natural frequencies and mode shapes on the GPU (FESystem.solve_modal, solver.py:2047-2114).
+
+The reference calls scipy.sparse.linalg.eigsh(Kff, k=n_modes, M=Mff, sigma=0): shift-invert
+Lanczos on a sparse LU factorisation.  feab200 finds the same lowest eigenpairs of
+K phi = lambda M phi by block subspace iteration (inverse iteration on a block of p > n_modes
+vectors) with a Rayleigh-Ritz step, every product on the GPU:
+
+    Y  = K^-1 (M X)                 block-PCG, one column per vector (feab_block_pcg_solve)
+    Kr = Y^T K Y,  Mr = Y^T M Y      CSR SpMVs (feab_csr_spmv) and FP64 cuBLAS GEMMs
+    Kr v = lambda Mr v               Mr = Q L Q^T, then the eigenpairs of L^-1/2 Q^T Kr Q L^-1/2
+                                     (feab_symeig_jacobi, one CTA, k <= 64)
+    X  = Y V                         M-orthonormal Ritz vectors, lambda ascending
+
+until the n_modes lowest Ritz values change by less than ``tol`` (relative).  Ritz values converge
+like (lambda_i / lambda_{p+1})^(2j), so the block is wider than the number of modes asked for.
+"""
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from .batched import block_pcg, panel_width
+from .device import ReducedOperator, spmv
+from .pod import symeig
+
+
+def _apply_columns(op: ReducedOperator, X):
+    """op @ X for an (n, p) device panel, one CSR SpMV per column."""
+    XT = X.t().contiguous()
+    out = torch.empty_like(XT)
+    for j in range(XT.shape[0]):
+        spmv(op, XT[j], "fp64", out=out[j])
+    return out.t()
+
+
+def _generalized_eig(Kr, Mr):
+    """Eigenpairs of Kr v = lambda Mr v (Kr, Mr symmetric, Mr positive definite), lambda ascending
+    and V^T Mr V = I."""
+    lm, Q = symeig(Mr)
+    if not bool((lm > 0).all()):
+        raise np.linalg.LinAlgError("solve_modal: the subspace lost rank (M-Gram matrix not positive definite)")
+    S = Q * lm.rsqrt()[None, :]
+    A = S.t() @ Kr @ S
+    A = 0.5 * (A + A.t())
+    w, W = symeig(A)
+    order = torch.argsort(w)
+    return w[order], S @ W[:, order]
+
+
+def subspace_iteration(Kop: ReducedOperator, Mop: ReducedOperator, n_modes, subspace=None, tol=1e-12, maxiter=300,
+                       pcg_tol=1e-10, seed=0):
+    """The n_modes lowest eigenpairs of Kff phi = lambda Mff phi.  Returns (lambda (n_modes,)
+    device, Phi (n, n_modes) device, M-orthonormal, iterations)."""
+    n = Kop.n
+    if not (1 <= n_modes < n):
+        raise ValueError(f"solve_modal: n_modes must be in [1, {n - 1}] for {n} free DOFs, got {n_modes}")
+    p = int(subspace) if subspace else max(2 * n_modes, n_modes + 8)
+    p = max(n_modes, min(p, n, 64))
+    K = panel_width(p)
+    dev = Kop.vals64.device
+    g = torch.Generator(device=dev).manual_seed(int(seed))
+    X = torch.randn((n, p), generator=g, dtype=torch.float64, device=dev)
+    B = torch.zeros((n, K), dtype=torch.float64, device=dev)
+    lam_old = None
+    for it in range(1, maxiter + 1):
+        B[:, :p] = _apply_columns(Mop, X)
+        Y, res = block_pcg(Kop, np.array([0, n]), B, [p], tol=pcg_tol)
+        if not (res.status == 0).all():
+            raise RuntimeError(f"solve_modal: the inner block-PCG did not converge (status {res.status.tolist()})")
+        Y = Y[:, :p]
+        Kr = Y.t() @ _apply_columns(Kop, Y)
+        Mr = Y.t() @ _apply_columns(Mop, Y)
+        lam, V = _generalized_eig(0.5 * (Kr + Kr.t()), 0.5 * (Mr + Mr.t()))
+        X = Y @ V
+        low = lam[:n_modes]
+        if lam_old is not None:
+            change = float(((low - lam_old).abs() / low.abs().clamp_min(1e-300)).max())
+            if change < tol:
+                break
+        lam_old = low.clone()
+    return lam[:n_modes], X[:, :n_modes].contiguous(), it

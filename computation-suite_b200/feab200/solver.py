@@ -65,6 +65,10 @@ class FESystem:
         self._stiffness_args = None
         self.last_solve_info = None
         self._bc_cache = None    # (frozenset of fixed DOFs, free, fixed, {device: (free_t, fixed_t)})
+        self._me = None          # packed consistent element mass matrices on the device (E, 324)
+        self._me_version = 0
+        self._mop_cache = None   # (key, ReducedOperator of M_ff)
+        self._M_full = None
 
     # ------------------------------------------------------------------ device objects
     @property
@@ -182,6 +186,72 @@ class FESystem:
         self._K_full = None
         self._assembled.add("K")
         self._stiffness_args = (D, {"thickness": thickness})
+
+    def assemble_mass(self, rho_or_matrix, accumulate=False, **kwargs):
+        """Consistent mass M = sum_e sum_q Nm^T R Nm |detJ| w thickness on the GPU (solver.py:699-740,
+        Element.mass, elements/base.py:711-731).  rho_or_matrix: the 3x3 density matrix of a solid
+        (rho * np.eye(3)); a scalar raises ValueError, as it does in the reference."""
+        thickness = kwargs.pop("thickness", 1.0)
+        if kwargs:
+            raise TypeError(f"assemble_mass: unsupported kwargs {list(kwargs)}")
+        if np.isscalar(rho_or_matrix):
+            raise ValueError(
+                f"assemble_mass: {type(self.elem).__name__}.mass() could not use the scalar density "
+                f"{rho_or_matrix!r}. This element needs a density MATRIX -- for a solid pass rho * np.eye(3).")
+        R = np.asarray(rho_or_matrix, dtype=float)
+        if R.shape != (3, 3):
+            raise ValueError(f"assemble_mass: the density matrix of a hex8 solid is 3x3, got shape {R.shape}")
+        if self._me is not None and not accumulate and "M" not in self._warned_reassembly:
+            warnings.warn("assemble_mass: M was already assembled, so it is being REPLACED. Pass accumulate=True "
+                          "to add to the existing matrix instead.", UserWarning, stacklevel=2)
+            self._warned_reassembly.add("M")
+        me = self.device_mesh.element_mass(R, thickness=thickness)
+        self._me = self._me + me if (accumulate and self._me is not None) else me
+        self._me_version += 1
+        self._mop_cache = None
+        self._M_full = None
+
+    @property
+    def M(self):
+        """Full (n_dof x n_dof) consistent mass as a host scipy CSR (None before assemble_mass)."""
+        if self._me is None:
+            return None
+        if self._M_full is None:
+            dm = self.device_mesh
+            self._M_full = dm.assemble(self._me, dm.pattern(()), want32=False).to_scipy()
+        return self._M_full
+
+    def reduced_mass_operator(self):
+        """M_ff for the current fixed set on the device, on the stiffness pattern."""
+        if self._me is None:
+            raise RuntimeError("call assemble_mass() first (the mass matrix M has not been assembled)")
+        fixed = self._bc_arrays()[2]
+        key = (self._me_version, fixed.tobytes())
+        if self._mop_cache is not None and self._mop_cache[0] == key:
+            return self._mop_cache[1]
+        dm = self.device_mesh
+        op = dm.assemble(self._me, dm.pattern(fixed), want32=False)
+        self._mop_cache = (key, op)
+        return op
+
+    def solve_modal(self, n_modes=4, tol=1e-12, maxiter=300, subspace=None, pcg_tol=1e-10):
+        """Natural frequencies (Hz) and M-orthonormal mode shapes of the constrained system
+        (solver.py:2047-2114).  The reference's shift-invert eigsh is replaced by GPU block
+        subspace iteration (feab200.modal).  Returns (freq_hz (n_modes,), FEField (n_dof, n_modes))."""
+        if self._me is None:
+            raise RuntimeError("call assemble_mass() first (the mass matrix M has not been assembled)")
+        self._require_stiffness("this solve")
+        from .modal import subspace_iteration
+        Kop = self.reduced_operator(want32=False)
+        Mop = self.reduced_mass_operator()
+        lam, Phi, iters = subspace_iteration(Kop, Mop, int(n_modes), subspace=subspace, tol=tol, maxiter=maxiter,
+                                             pcg_tol=pcg_tol)
+        self.last_modal_iterations = iters
+        lam = lam.clamp_min(0.0)
+        modes = torch.zeros((self.n_dof, int(n_modes)), dtype=torch.float64, device=self.device)
+        modes[self._bc_device_index()[0]] = Phi
+        freq = (lam.sqrt() / (2 * np.pi)).cpu().numpy()
+        return freq, self.field(modes.cpu().numpy(), label="mode shapes")
 
     def _require_stiffness(self, who):
         if self._ke is None:

@@ -195,6 +195,16 @@ int32_t feab_hex8_bbar_element_stiffness(const double* coords, const int32_t* co
                                          double* ke_out, int32_t layout, feab_device_status* status,
                                          cudaStream_t stream);
 
+/* Consistent mass of every element (Element.mass, elements/base.py:711-731, through
+ * FESystem.assemble_mass, solver.py:699-740): me = sum_q Nm^T R Nm |detJ| w thickness (times
+ * scale[e] when scale != NULL), i.e. node block (a, b) = m_ab R thickness with
+ * m_ab = sum_q N_a N_b |detJ| w.  R_host: the 3x3 density matrix (9 doubles, HOST memory,
+ * symmetric, e.g. rho I).  Same layouts as feab_hex8_element_stiffness, so feab_assemble_csr
+ * assembles M on the stiffness pattern. */
+int32_t feab_hex8_element_mass(const double* coords, const int32_t* conn, int64_t n_elem, const double* R_host,
+                               const double* scale, double thickness, double* me_out, int32_t layout,
+                               feab_device_status* status, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- assembly
  * Deterministic gather assembly of the reduced CSR values from packed element
  * matrices: each entry is summed over its elements in ascending element order.

@@ -17,7 +17,7 @@ import scipy.sparse.linalg as spla
 
 __all__ = [
     "gauss_legendre", "box_mesh", "perturb_interior", "D_solid3d", "hex8_shape_and_derivs",
-    "hex8_element_stiffness", "hex8_bbar_element_stiffness", "global_dofs", "structural_csr", "reduce_free", "fixed_dofs_on_plane",
+    "hex8_element_stiffness", "hex8_bbar_element_stiffness", "hex8_element_mass", "modal", "global_dofs", "structural_csr", "reduce_free", "fixed_dofs_on_plane",
     "free_dofs", "quad4_shape_and_derivs", "HEX8_FACES", "facet_load_shares", "facet_mass",
     "jacobi_inverse_diagonal", "preconditioned_cg", "simp_scale", "simp_scale_grad",
     "compliance_sensitivity_closed_form", "pod_singular_values", "element_strain_energy_density",
@@ -159,6 +159,33 @@ def hex8_element_stiffness(coords, D, thickness=1.0):
         B = _b_matrices(dN_g)
         ke += np.matmul(np.transpose(B, (0, 2, 1)), np.matmul(D, B)) * (detJ * w * thickness)[:, None, None]
     return ke
+
+
+def hex8_element_mass(coords, R, thickness=1.0):
+    """Consistent element mass me = sum_gp Nm^T R Nm |detJ| w thickness (Element.mass,
+    fea_engine/src/fea_engine/elements/base.py:711-731; Nm the 3 x 24 block expansion of N, N_matrix
+    :475-487).  coords (E, 8, 3), R the 3x3 density matrix.  Returns (E, 24, 24)."""
+    coords = np.asarray(coords, dtype=float)
+    R = np.asarray(R, dtype=float)
+    me = np.zeros((coords.shape[0], 24, 24))
+    pts, _ = _gauss_product_3d(2)
+    for (w, detJ, _), p in zip(_gauss_geometry(coords), pts):
+        N, _ = hex8_shape_and_derivs(*p)
+        Nm = np.zeros((3, 24))
+        for a in range(8):
+            Nm[:, 3 * a:3 * a + 3] = N[a] * np.eye(3)
+        me += (Nm.T @ R @ Nm)[None, :, :] * (np.abs(detJ) * w * thickness)[:, None, None]
+    return me
+
+
+def modal(Kff, Mff, n_modes):
+    """Lowest eigenpairs of Kff phi = w^2 Mff phi by shift-invert Lanczos, as FESystem.solve_modal
+    (solver.py:2047-2114): scipy.sparse.linalg.eigsh(Kff, k, M=Mff, sigma=0).  Returns
+    (freq_hz (n_modes,), modes (n_free, n_modes), M-orthonormal)."""
+    w2, vecs = spla.eigsh(sp.csc_matrix(Kff), k=n_modes, M=sp.csc_matrix(Mff), sigma=0, which="LM")
+    order = np.argsort(w2)
+    w2, vecs = np.clip(w2[order], 0, None), vecs[:, order]
+    return np.sqrt(w2) / (2 * np.pi), vecs
 
 
 def hex8_bbar_element_stiffness(coords, D, thickness=1.0):

@@ -28,6 +28,8 @@ simp_6x3x3.npz         SIMP compliance: densities, forward solution, closed-form
 pod_small.npz          singular values of a 400x12 snapshot matrix from PodBasis.fit.
 recovery_20x4x4.npz    the cantilever_20x4x4 system at its SuperLU displacement: FESystem.stress /
                        strain / von_mises at the nodes and per element, and reactions.
+modal_20x4x4.npz       Hex8Solid3D.mass of distorted hexes, and the cantilever_20x4x4 system's
+                       assemble_mass(7850 I) + solve_modal(n_modes=6).
 bbar_hex8.npz          Hex8SolidBbar element stiffness of distorted hexes (nu 0.3, 0.4999) and the
                        near-incompressible cantilever deflection with Hex8SolidBbar and Hex8Solid3D.
 topopt_8x4x4.npz       SIMP on an 8x4x4 cantilever: build_filter_weights, apply_sensitivity_filter,
@@ -296,6 +298,24 @@ def bbar_hex8():
     return out
 
 
+def modal_20x4x4():
+    """Consistent mass and the modal solve of the jittered 20x4x4 cantilever: Hex8Solid3D.mass of
+    6 distorted hexes (rho = 7850 I), and FESystem(sparse=True).assemble_mass(7850 I) +
+    solve_modal(n_modes=6) (shift-invert eigsh)."""
+    from fea_engine.elements.solids import Hex8Solid3D
+    fs, mesh, D, _ = _cantilever_20x4x4_system()
+    R = 7850.0 * np.eye(3)
+    rng = np.random.default_rng(23)
+    cube = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0], [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], float)
+    coords = np.stack([cube * rng.uniform(0.3, 2.0, 3) + 0.1 * rng.standard_normal((8, 3)) for _ in range(6)])
+    me = np.stack([Hex8Solid3D().mass(c, R) for c in coords])
+    fs.assemble_mass(R)
+    freq, modes = fs.solve_modal(n_modes=6)
+    return dict(coords=coords, R=R, me=me, nodes=np.asarray(mesh.nodes), elements=np.asarray(mesh.elements, np.int64),
+                D=D, fixed=np.asarray(fs.fixed_dofs_array), freq=np.asarray(freq), modes=np.asarray(modes),
+                M_nnz=np.int64(fs.M.tocsr().nnz if hasattr(fs.M, "tocsr") else np.count_nonzero(fs.M)))
+
+
 def pod_small():
     from rom_engine.pod import PodBasis
     rng = np.random.default_rng(3)
@@ -315,7 +335,7 @@ def main():
     for name, fn in [("cantilever_20x4x4", cantilever_20x4x4), ("pattern_4x3x2", pattern_4x3x2),
                      ("ke_distorted", ke_distorted), ("facets", facets), ("simp_6x3x3", simp_6x3x3),
                      ("pod_small", pod_small), ("recovery_20x4x4", recovery_20x4x4),
-                     ("topopt_8x4x4", topopt_8x4x4), ("bbar_hex8", bbar_hex8)]:
+                     ("topopt_8x4x4", topopt_8x4x4), ("bbar_hex8", bbar_hex8), ("modal_20x4x4", modal_20x4x4)]:
         if args.only and name not in args.only:
             continue
         data = fn()

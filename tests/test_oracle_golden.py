@@ -142,3 +142,18 @@ def test_bbar_element_stiffness_matches_reference(golden):
     for tag in ("03", "04999"):
         ke = O.hex8_bbar_element_stiffness(g["coords"], g["D_" + tag])
         assert _relnorm(ke, g["ke_" + tag]) < 1e-14
+
+
+def test_mass_and_modal_match_reference(golden):
+    g = golden("modal_20x4x4")
+    assert _relnorm(O.hex8_element_mass(g["coords"], g["R"]), g["me"]) < 1e-14
+    X, el = g["nodes"], g["elements"]
+    free = O.free_dofs(3 * len(X), g["fixed"])
+    Kff = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(X[el], g["D"]), el, 3 * len(X)), free)
+    Mff = O.reduce_free(O.structural_csr(O.hex8_element_mass(X[el], g["R"]), el, 3 * len(X)), free)
+    f, V = O.modal(Kff, Mff, 6)
+    assert np.max(np.abs(f - g["freq"]) / g["freq"]) < 1e-10
+    # M-orthonormal modes spanning the reference's subspace
+    Vr = g["modes"][free]
+    assert np.allclose(V.T @ (Mff @ V), np.eye(6), atol=1e-8)
+    assert np.linalg.norm(Vr - V @ (V.T @ (Mff @ Vr))) / np.linalg.norm(Vr) < 1e-6

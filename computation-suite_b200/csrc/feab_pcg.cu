@@ -408,7 +408,7 @@ __global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
 // Sliced path, kernel A: Ap = K p and p.Ap through the SELL-32 operator (PREC = its kind); in a
 // mixed reliable step, the FP64 residual r = b - K64 x through the CSR values instead.
 template <int PREC>
-__global__ void __launch_bounds__(kThreads, FEAB_SELL_MINB) k_step_a_sell(PcgArgs A) {
+__global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step_a_sell(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;

@@ -176,7 +176,7 @@ __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, FEAB_SELL_MINB) k_sell_spmv(SellView V, const double* __restrict__ x,
+__global__ void __launch_bounds__(kThreads, SellTuning<KIND>::kMinBlocks) k_sell_spmv(SellView V, const double* __restrict__ x,
                                                            double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
   const int nw = (gridDim.x * blockDim.x) >> 5;

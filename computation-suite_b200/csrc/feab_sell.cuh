@@ -19,9 +19,12 @@
 #ifndef FEAB_SELL_PREFETCH
 #define FEAB_SELL_PREFETCH 0
 #endif
-// Blocks of 4 steps whose loads a lane issues before it consumes any.
-#ifndef FEAB_SELL_BLOCKS
-#define FEAB_SELL_BLOCKS 2
+// Blocks of 4 steps whose loads a lane issues before it consumes any, per operator kind.
+#ifndef FEAB_SELL_BLOCKS_FP64
+#define FEAB_SELL_BLOCKS_FP64 2
+#endif
+#ifndef FEAB_SELL_BLOCKS_MIXED
+#define FEAB_SELL_BLOCKS_MIXED 1
 #endif
 // 1: load the operator with the streaming (evict-first) cache hint, so that the CG vectors
 // (a few MB, re-read every iteration) stay in L2 while K streams through it.
@@ -33,9 +36,15 @@
 #ifndef FEAB_SELL_FUSED_P
 #define FEAB_SELL_FUSED_P 0
 #endif
-// Minimum resident 256-thread CTAs per SM for the sliced SpMV kernels (register budget).
-#ifndef FEAB_SELL_MINB
-#define FEAB_SELL_MINB 2
+// Minimum resident 256-thread CTAs per SM for the sliced SpMV kernels (register budget), per
+// operator kind.  Measured in the PCG at 128x32x32: the 48-bit kernel runs 54.4 us per iteration
+// at 4 CTAs with one block in flight against 57.5 us at 2 CTAs with two; the FP64 kernel is
+// fastest at 2 CTAs with two blocks.
+#ifndef FEAB_SELL_MINB_FP64
+#define FEAB_SELL_MINB_FP64 2
+#endif
+#ifndef FEAB_SELL_MINB_MIXED
+#define FEAB_SELL_MINB_MIXED 4
 #endif
 
 namespace feab {
@@ -86,6 +95,13 @@ __device__ __forceinline__ double sell_dec48(uint32_t hi, uint16_t lo) {
   return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
 }
 
+// Per-kind load depth and register budget of the sliced SpMV kernels.
+template <int KIND>
+struct SellTuning {
+  static constexpr int kBlocks = KIND == FEAB_PREC_FP64 ? FEAB_SELL_BLOCKS_FP64 : FEAB_SELL_BLOCKS_MIXED;
+  static constexpr int kMinBlocks = KIND == FEAB_PREC_FP64 ? FEAB_SELL_MINB_FP64 : FEAB_SELL_MINB_MIXED;
+};
+
 // acc[k] = (K x)[r0 + k] for the lane's group, x read through xf(column).  Mixed kind: the
 // difference form sum_{b != a} w (x_b - x_a) + S x_a, evaluated as sum_{b != a} w x_b + T x_a
 // with T = S - sum_{b != a} w precomputed (the same value exactly, so the same rounding error of
@@ -93,6 +109,7 @@ __device__ __forceinline__ double sell_dec48(uint32_t hi, uint16_t lo) {
 template <int KIND, typename XF>
 __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lane, const SellLane& L, XF xf,
                                            double (&acc)[3], double (&xs)[3]) {
+  constexpr int NB = SellTuning<KIND>::kBlocks;
   const int base = __ldg(V.soff + slice), W = __ldg(V.soff + slice + 1) - base;
   double a0 = 0.0, a1 = 0.0, a2 = 0.0;
 #pragma unroll
@@ -115,16 +132,16 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
   };
 #pragma unroll
   for (int i = 1; i < FEAB_SELL_PREFETCH; ++i) prefetch_block(4 * i);
-  for (int j = 0; j < W; j += 4 * FEAB_SELL_BLOCKS) {
+  for (int j = 0; j < W; j += 4 * NB) {
     prefetch_block(j + 4 * FEAB_SELL_PREFETCH);
-    // all loads of FEAB_SELL_BLOCKS blocks first (a block past the slice end is skipped; W is
+    // all loads of NB blocks first (a block past the slice end is skipped; W is
     // the same for the whole warp, so the test does not diverge)
-    unsigned t[FEAB_SELL_BLOCKS][4];
-    double v[KIND == FEAB_PREC_FP64 ? FEAB_SELL_BLOCKS : 1][3][4];
-    uint4 h[KIND == FEAB_PREC_FP64 ? 1 : FEAB_SELL_BLOCKS][3];
-    uint2 l[KIND == FEAB_PREC_FP64 ? 1 : FEAB_SELL_BLOCKS][3];
+    unsigned t[NB][4];
+    double v[KIND == FEAB_PREC_FP64 ? NB : 1][3][4];
+    uint4 h[KIND == FEAB_PREC_FP64 ? 1 : NB][3];
+    uint2 l[KIND == FEAB_PREC_FP64 ? 1 : NB][3];
 #pragma unroll
-    for (int nb = 0; nb < FEAB_SELL_BLOCKS; ++nb) {
+    for (int nb = 0; nb < NB; ++nb) {
       if (nb > 0 && j + 4 * nb >= W) break;
       const size_t b = (size_t)(base + j + 4 * nb);
       const uint4 tq = ld_op(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
@@ -152,7 +169,7 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
       }
     }
 #pragma unroll
-    for (int nb = 0; nb < FEAB_SELL_BLOCKS; ++nb) {
+    for (int nb = 0; nb < NB; ++nb) {
       if (nb > 0 && j + 4 * nb >= W) break;
       if (KIND == FEAB_PREC_FP64) {
 #pragma unroll

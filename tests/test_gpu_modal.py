@@ -77,3 +77,11 @@ def test_solve_modal_requires_mass():
     fs.fix_dofs(g_mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
     with pytest.raises(RuntimeError):
         fs.solve_modal(2)
+
+
+def test_solve_modal_rejects_bad_mode_counts(system):
+    fs, g = system
+    with pytest.raises(ValueError):
+        fs.solve_modal(0)
+    with pytest.raises(ValueError):
+        fs.solve_modal(len(fs.free_dofs))

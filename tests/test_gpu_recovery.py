@@ -87,3 +87,27 @@ def test_recovery_error_paths(system):
         fs.von_mises(g["U"], plane="strain")
     with pytest.raises(ValueError):
         fs.device_mesh.recover(g["U"], None, von_mises=True)
+
+
+def test_recovery_rejects_bad_inputs():
+    import ctypes as C
+    import torch
+    from feab200 import _lib as L
+    from feab200.device import DeviceMesh
+    nodes, el = O.box_mesh(1.0, 1.0, 1.0, 2, 2, 2)
+    dm = DeviceMesh(nodes, el)
+    topo = dm.topology()
+    u = torch.zeros(3 * len(nodes), dtype=torch.float64, device=dm.device)
+    sb = int(L.lib.feab_hex8_recover_scratch_bytes(dm.n_elem))
+    scratch = torch.empty(sb, dtype=torch.uint8, device=dm.device)
+    out = torch.empty((len(nodes), 6), dtype=torch.float64, device=dm.device)
+    args = lambda n_elem, sbytes, nodal: (L.dptr(dm.coords), L.dptr(dm.conn), n_elem, len(nodes),  # noqa: E731
+                                           L.dptr(topo.inc_ptr), L.dptr(topo.inc_elem), None, L.dptr(u), nodal, None,
+                                           None, None, L.dptr(scratch), sbytes, None, dm.stream)
+    assert L.lib.feab_hex8_recover(*args(0, sb, L.dptr(out))) == L.FEAB_BAD_ARG          # no elements
+    assert L.lib.feab_hex8_recover(*args(dm.n_elem, sb - 8, L.dptr(out))) == L.FEAB_BAD_ARG   # scratch too small
+    assert L.lib.feab_hex8_recover(*args(dm.n_elem, sb, None)) == L.FEAB_BAD_ARG          # no output asked for
+    assert L.lib.feab_hex8_recover(*args(dm.n_elem, sb, C.c_void_p(out.data_ptr() + 8))) == L.FEAB_BAD_ARG  # misaligned
+    assert L.lib.feab_hex8_recover(*args(dm.n_elem, sb, L.dptr(out))) == L.FEAB_OK
+    torch.cuda.synchronize()
+    assert float(out.abs().max()) == 0.0                                                   # u = 0 -> no strain

@@ -92,3 +92,20 @@ def test_unknown_sensitivity_rejected(case):
     fs, g = case
     with pytest.raises(ValueError, match="unknown sensitivity"):
         topopt.topology_optimize_compliance(fs, g["D"], g["F"], 0.4, sensitivity="bogus", n_iter=1)
+
+
+def test_filter_with_only_self_neighbours_is_identity_and_bad_inputs_raise():
+    from feab200 import topopt
+    rng = np.random.default_rng(4)
+    cent = rng.uniform(0, 1, (50, 3)) * 10.0                 # points much farther apart than the radius
+    H = topopt.build_filter_weights(cent, 1e-6)
+    assert H.nnz == 50 and np.allclose(np.diag(H.toarray()), 1e-6)
+    rho, dc = rng.uniform(0.1, 1.0, 50), -rng.uniform(0.1, 1.0, 50)
+    assert np.allclose(topopt.apply_sensitivity_filter(H, rho, dc), dc, rtol=1e-15, atol=0)
+    with pytest.raises(ValueError):
+        topopt.build_filter_weights(cent, 0.0)
+    with pytest.raises(ValueError):
+        topopt.oc_update(np.zeros(0), np.zeros(0), 0.4)
+    # dc all positive (clipped to -1e-12) still gives finite densities inside the bounds
+    r = topopt.oc_update(np.full(10, 0.5), np.full(10, 1.0), 0.5)
+    assert np.all(np.isfinite(r)) and np.all((r >= 1e-3) & (r <= 1.0))

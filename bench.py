@@ -296,6 +296,29 @@ def spmv_roofline(op, precision, reps, peak_gbs):
             "csr_formula_bytes": int(bytes_csr), "launch_us": round(t * 1e6, 2)}
 
 
+def pcg_iteration_roofline(op, b, tol, precision, peak_gbs):
+    """The whole PCG iteration as one unit: a full solve timed with CUDA events on the solve's
+    stream, divided by its iterations, against the iteration's algorithmic bytes: the SpMV of
+    spmv_bytes (which counts reading p once and writing Ap), plus P (reads z and p, writes p),
+    A's own p rows for p.Ap, and B (reads x, p, r, Ap and dinv, writes x, r and z): 12 n doubles."""
+    import torch
+    from feab200.device import pcg_solve
+    pcg_solve(op, b, tol=tol, precision=precision)
+    torch.cuda.synchronize()
+    a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record()
+    _, info = pcg_solve(op, b, tol=tol, precision=precision)
+    e.record()
+    torch.cuda.synchronize()
+    t = a.elapsed_time(e) * 1e-3 / max(1, info.iters)
+    nbytes = spmv_bytes(op, precision) + 12 * op.n * 8
+    return {"us_per_iteration": round(t * 1e6, 2), "iterations": info.iters, "bytes_per_iteration": int(nbytes),
+            "achieved": round(nbytes / t / 1e9, 1), "peak": peak_gbs, "unit": "GB/s",
+            "frac": round(nbytes / t / 1e9 / peak_gbs, 3),
+            "note": "solve time (operator build and setup included) over its iterations; the SpMV step kernel "
+                    "dominates"}
+
+
 class L2Flush:
     """Evicts L2 before a timed launch: writes one 256 MB buffer (twice the 126 MB L2), then reads
     a second one, so that the dirty lines of the write are written back before the timed kernel
@@ -941,6 +964,8 @@ def main():
             roof["traffic_kernel"] = t["kernel"]
     except (OSError, ValueError, KeyError):
         pass
+    pcg_iter = {prec: pcg_iteration_roofline(o, prob.Ff, args.tol, prec, peak)
+                for prec, o in (("mixed", op), ("fp64", op64))}
     e2e_ms, h2d, d2h = e2e_steps(c, "mixed", args.tol, args.e2e_steps, 1)
     e2e_ms = max_over_ranks(e2e_ms, world)
     cpu = None
@@ -965,6 +990,7 @@ def main():
                         "dc_mixed_vs_fp64": dc_err, "tight_tol": 1e-13, "mixed_relres_fp64": info32.relres},
             "roofline": roof,
             "roofline_fp64": roof64,
+            "pcg_iteration": pcg_iter,
             "cpu_baseline": cpu,
             "e2e": {"value": round(e2e_ms, 2), "unit": "ms", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "path": "FESystem + topopt from host numpy (pageable) arrays"},

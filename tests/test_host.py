@@ -86,3 +86,39 @@ def test_batch_and_snapshot_builders_are_seeded():
     s = cl.fourier_snapshot_cantilever(nx=4, ny=3, nz=3, n_rhs=5)
     tip_t = s.F[2::3]
     assert s.F.shape == (3 * len(s.mesh.nodes), 5) and np.abs(tip_t).max() > 0
+
+
+def test_fixed_dof_bookkeeping_is_cached_and_follows_direct_edits():
+    """fix_dofs records DOFs node-major like the reference's loop (solver.py:1109-1176), and the
+    cached free / fixed arrays follow every change of the fixed set, including direct edits."""
+    m = box_mesh(1.0, 0.5, 0.5, 4, 2, 2)
+    fs = FESystem(m, Hex8Solid3D())
+    nodes = m.nodes_on_plane(0, 0.0)
+    fs.fix_dofs(nodes, [2, 0], value=0.25)
+    expected = [3 * int(n) + k for n in nodes for k in (2, 0)]
+    assert list(fs.fixed_dof_values) == expected
+    assert set(fs.fixed_dof_values.values()) == {0.25}
+    fixed = fs.fixed_dofs_array
+    assert np.array_equal(fixed, np.sort(expected))
+    assert np.array_equal(fs.free_dofs, np.setdiff1d(np.arange(fs.n_dof), expected))
+    assert np.array_equal(fs._fixed_dof_values_array(fixed), np.full(len(fixed), 0.25))
+    # the returned arrays are copies: editing them does not touch the cache
+    f = fs.free_dofs
+    f[:] = -1
+    assert fs.free_dofs.min() >= 0
+    # a direct edit of the set is seen; a DOF without a recorded value counts as 0
+    fs.fixed_dofs.add(1)
+    assert 1 not in fs.free_dofs and 1 in fs.fixed_dofs_array
+    assert fs._fixed_dof_values_array(np.array([1]))[0] == 0.0
+    fs.fixed_dofs.discard(1)
+    assert 1 in fs.free_dofs
+    with pytest.raises(ValueError):
+        fs.fix_dofs([len(m.nodes)], [0])
+    with pytest.raises(ValueError):
+        fs.fix_dofs(nodes, [3])
+
+
+def test_bench_byte_counts():
+    """The algorithmic byte formulas the bench's rooflines divide by."""
+    import bench
+    assert bench.recovery_bytes(10, 4) == 4 * (32 + 448 + 56 + 32 + 32 + 448) + 10 * (48 + 4 + 56)

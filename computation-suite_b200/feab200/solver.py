@@ -69,6 +69,7 @@ class FESystem:
         self._me_version = 0
         self._mop_cache = None   # (key, ReducedOperator of M_ff)
         self._M_full = None
+        self.last_modal_iterations = None
 
     # ------------------------------------------------------------------ device objects
     @property

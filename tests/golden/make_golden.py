@@ -29,7 +29,10 @@ pod_small.npz          singular values of a 400x12 snapshot matrix from PodBasis
 recovery_20x4x4.npz    the cantilever_20x4x4 system at its SuperLU displacement: FESystem.stress /
                        strain / von_mises at the nodes and per element, and reactions.
 modal_20x4x4.npz       Hex8Solid3D.mass of distorted hexes, and the cantilever_20x4x4 system's
-                       assemble_mass(7850 I) + solve_modal(n_modes=6).
+                       assemble_mass(7850 I) + solve_modal(n_modes=6).  The frequencies reproduce
+                       run to run; the mode vectors' signs and their rotation inside the two
+                       near-degenerate bending pairs follow ARPACK's random start vector, so the
+                       tests compare the spanned subspace, not the vectors.
 bbar_hex8.npz          Hex8SolidBbar element stiffness of distorted hexes (nu 0.3, 0.4999) and the
                        near-incompressible cantilever deflection with Hex8SolidBbar and Hex8Solid3D.
 topopt_8x4x4.npz       SIMP on an 8x4x4 cantilever: build_filter_weights, apply_sensitivity_filter,

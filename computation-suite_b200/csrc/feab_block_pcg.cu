@@ -877,6 +877,9 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   if (prec != FEAB_PREC_FP64 && prec != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
   if (prec == FEAB_PREC_MIXED && !D) return FEAB_BAD_ARG;
   if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return FEAB_BAD_ARG;  // 16-byte panel gathers
+  // the R / P / AP panels are carved from the workspace at 256-byte offsets and are read and
+  // written with 16-byte accesses by the vector passes
+  if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return FEAB_BAD_ARG;
   const BLayout L = blayout(M->n, k, bt->n_problems, bt->n_items);
   if (L.total > workspace_bytes) return FEAB_BAD_ARG;
   char* w = static_cast<char*>(workspace);

@@ -302,7 +302,7 @@ int32_t feab_csr_spmv(const feab_csr* A, const feab_sell_operator* sell, int32_t
  * runs its own CG recurrence (preconditioned_cg, iterative_solvers.py:434-481) -- the
  * iterative counterpart of solve_batched / solve_static_batched (batched_solve.py:44-164),
  * which factorise once for many columns.  precision: FEAB_PREC_FP64 or FEAB_PREC_MIXED
- * (diff != NULL).  X must be 16-byte aligned.  Synchronous; per-column iterations / FP64
+ * (diff != NULL).  X and the workspace must be 16-byte aligned.  Synchronous; per-column iterations / FP64
  * relative residuals and per-problem status go to the optional host arrays. */
 typedef struct feab_batch {
   int32_t n_problems;

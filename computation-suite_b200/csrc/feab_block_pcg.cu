@@ -880,6 +880,9 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   // the R / P / AP panels are carved from the workspace at 256-byte offsets and are read and
   // written with 16-byte accesses by the vector passes
   if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return FEAB_BAD_ARG;
+  if (D && (!D->tcol || !D->vhi || !D->vlo || (reinterpret_cast<uintptr_t>(D->tcol) & 15) ||
+            (reinterpret_cast<uintptr_t>(D->vhi) & 15) || (reinterpret_cast<uintptr_t>(D->vlo) & 7)))
+    return FEAB_BAD_ARG;  // 16-byte column / hi-word quads, 8-byte lo words
   const BLayout L = blayout(M->n, k, bt->n_problems, bt->n_items);
   if (L.total > workspace_bytes) return FEAB_BAD_ARG;
   char* w = static_cast<char*>(workspace);

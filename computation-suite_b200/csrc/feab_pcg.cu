@@ -958,10 +958,14 @@ void fill_sell(const feab_csr* M, const feab_sell_operator* D, PcgArgs* A) {
   A->use_sell = 1;
 }
 
-// A sliced operator fits A and is of the kind the precision needs.
+// A sliced operator fits A, is of the kind the precision needs, and its arrays have the alignment
+// of the SpMV's vector loads (16 bytes; 8 for the 16-bit lo words).
 bool sell_fits(const feab_csr* M, const feab_sell_operator* D, int kind) {
+  auto al = [](const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; };
   return D && M->group_ptr && M->n_groups > 0 && D->kind == kind && D->n_slices == (M->n_groups + 31) / 32 &&
-         D->soff && D->tcol && (kind == FEAB_PREC_FP64 ? D->v64 != nullptr : (D->vhi && D->vlo && D->gmask && D->S));
+         D->soff && D->tcol && al(D->tcol, 16) &&
+         (kind == FEAB_PREC_FP64 ? (D->v64 != nullptr && al(D->v64, 16))
+                                 : (D->vhi && D->vlo && D->gmask && D->S && al(D->vhi, 16) && al(D->vlo, 8)));
 }
 
 // Upper bounds from the sizes: sum_g Lp_g <= sum_g (len_g - f_g + 3) <= nnz + 3 G (f_g >= 1) and
@@ -1028,6 +1032,7 @@ extern "C" int32_t feab_diff_operator_build(const feab_csr* M, const int32_t* do
                                             size_t storage_bytes, feab_diff_operator* out, cudaStream_t s) {
   if (!M || !dof_of || !storage || !out || !M->group_ptr || M->n_groups <= 0 || !M->vals64 || M->n <= 0)
     return FEAB_BAD_ARG;
+  if (reinterpret_cast<uintptr_t>(storage) & 15u) return FEAB_BAD_ARG;  // 16-byte quad loads of the operator
   if (M->n >= (1 << 30) || M->nnz + 3 * (int64_t)M->n_groups >= (int64_t)INT32_MAX) return FEAB_CAPACITY;
   if (feab_diff_operator_bytes(M->n, M->nnz, M->n_groups) > storage_bytes) return FEAB_BAD_ARG;
   DiffScratch X;

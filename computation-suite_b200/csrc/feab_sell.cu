@@ -235,6 +235,7 @@ extern "C" int32_t feab_sell_operator_build(const feab_csr* A, const int32_t* do
     return FEAB_BAD_ARG;
   if (kind != FEAB_PREC_FP64 && kind != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
   if (kind == FEAB_PREC_MIXED && !dof_of) return FEAB_BAD_ARG;
+  if (reinterpret_cast<uintptr_t>(storage) & 15u) return FEAB_BAD_ARG;  // the SpMV's 16-byte loads
   if (A->n >= (1 << 30)) return FEAB_CAPACITY;
   const int32_t ns = (A->n_groups + 31) / 32;
   if ((int64_t)ns * round4(max_row_len) * 96 >= ((int64_t)1 << 40)) return FEAB_CAPACITY;
@@ -267,6 +268,11 @@ extern "C" int32_t feab_sell_spmv(const feab_csr* A, const feab_sell_operator* o
   if (!A || !op || !x || !y || !A->group_ptr || A->n_groups <= 0 || op->n_slices != (A->n_groups + 31) / 32)
     return FEAB_BAD_ARG;
   if (op->kind != FEAB_PREC_FP64 && op->kind != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
+  auto al = [](const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; };
+  if (!op->soff || !op->tcol || !al(op->tcol, 16)) return FEAB_BAD_ARG;
+  if (op->kind == FEAB_PREC_FP64 ? (!op->v64 || !al(op->v64, 16))
+                                 : (!op->vhi || !op->vlo || !op->gmask || !op->S || !al(op->vhi, 16) || !al(op->vlo, 8)))
+    return FEAB_BAD_ARG;
   launch_sell_spmv(sell_view(A, op), x, y, s);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;

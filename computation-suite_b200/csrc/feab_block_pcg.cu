@@ -25,6 +25,7 @@
 #include <algorithm>
 #include <cmath>
 #include "feab_common.cuh"
+#include "feab_graph.cuh"
 
 namespace feab {
 namespace {
@@ -769,10 +770,10 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   k_bsetup<K><<<grid, kThreads, 0, s>>>(A);
   count_launches(1);
   if (cudaGetLastError() != cudaSuccess) return FEAB_CUDA_ERROR;
-  int32_t* hflag = nullptr;
-  if (cudaHostAlloc((void**)&hflag, 64, cudaHostAllocDefault) != cudaSuccess) return FEAB_CUDA_ERROR;
-  cudaStream_t cs = nullptr;
-  cudaGraph_t graph = nullptr;
+  static thread_local HostFlag flag;
+  static thread_local GraphCache graphs;
+  if (!flag.ptr) return FEAB_CUDA_ERROR;
+  volatile int32_t* hflag = flag.ptr;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int32_t rc = FEAB_OK;
@@ -781,24 +782,22 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
     return e != cudaSuccess;
   };
   do {
-    if (fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking))) break;
-    if (fail(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming))) break;
-    if (fail(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) break;
-    if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
-    for (int q = 0; q < chunk; ++q) {
-      if (prec == FEAB_PREC_MIXED) {
-        k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
-        k_bstep_a<K, true><<<grid, kThreads, 0, cs>>>(A);
-        k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
-      } else {
-        k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
-        k_bstep_a<K, false><<<grid, kThreads, 0, cs>>>(A);
-        k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
+    if (fail(graphs.events(ev))) break;
+    auto record = [&](cudaStream_t cs) {
+      for (int q = 0; q < chunk; ++q) {
+        if (prec == FEAB_PREC_MIXED) {
+          k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_a<K, true><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
+        } else {
+          k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_a<K, false><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
+        }
       }
-    }
-    cudaMemcpyAsync(hflag, A.remaining, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
-    if (fail(cudaStreamEndCapture(cs, &graph))) break;
-    if (fail(cudaGraphInstantiate(&exec, graph, 0))) break;
+      cudaMemcpyAsync((void*)hflag, A.remaining, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
+    };
+    if (fail(graphs.acquire(&A, sizeof(A), topo_signature({K, prec, chunk, grid}), record, &exec))) break;
     // iterations and reliable steps per problem are bounded by maxiter each
     const int64_t max_launch = (2 * (int64_t)maxiter + 2 + chunk - 1) / chunk + 1;
     hflag[0] = np;
@@ -844,12 +843,6 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
     free(hp);
     free(hc);
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  if (ev[0]) cudaEventDestroy(ev[0]);
-  if (ev[1]) cudaEventDestroy(ev[1]);
-  if (cs) cudaStreamDestroy(cs);
-  cudaFreeHost(hflag);
   return worst;
 }
 

@@ -28,8 +28,8 @@
 //                    folding the correction into an FP64 solution.
 #include <algorithm>
 #include <cmath>
-#include <mutex>
 #include "feab_common.cuh"
+#include "feab_graph.cuh"
 #include "feab_scan.cuh"
 #include "feab_sell.cuh"
 
@@ -802,17 +802,6 @@ size_t layout(int32_t n, int32_t precision, char* base, PcgArgs* A) {
   return off;
 }
 
-struct HostFlag {
-  volatile int32_t* ptr = nullptr;
-  HostFlag() {
-    void* p = nullptr;
-    if (cudaHostAlloc(&p, 64, cudaHostAllocDefault) == cudaSuccess) ptr = static_cast<volatile int32_t*>(p);
-  }
-  ~HostFlag() {
-    if (ptr) cudaFreeHost((void*)ptr);
-  }
-};
-
 template <int PREC>
 void launch_setup(const PcgArgs& A, const Grids& gr, int lpg, cudaStream_t s) {
   if (lpg == 4) k_setup_a<PREC, 4><<<gr.a, kThreads, 0, s>>>(A);
@@ -857,8 +846,7 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
   else launch_setup<FEAB_PREC_FP64>(A, gr, lpg, s);
   FEAB_CHECK_LAUNCH();
 
-  cudaStream_t cs = nullptr;
-  cudaGraph_t graph = nullptr;
+  static thread_local GraphCache graphs;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int32_t rc = FEAB_OK;
@@ -868,19 +856,20 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
     return e != cudaSuccess;
   };
   do {
-    if (fail(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking))) break;
-    if (fail(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming))) break;
-    if (fail(cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming))) break;
-    if (fail(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal))) break;
-    for (int c = 0; c < chunk; ++c) {
-      if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, lpg, cs);
-      else if (prec == FEAB_PREC_MIXED) launch_step_sell<FEAB_PREC_MIXED>(A, gr, cs);
-      else if (A.use_sell) launch_step_sell<FEAB_PREC_FP64>(A, gr, cs);
-      else launch_step<FEAB_PREC_FP64>(A, gr, lpg, cs);
-    }
-    cudaMemcpyAsync((void*)flag.ptr, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
-    if (fail(cudaStreamEndCapture(cs, &graph))) break;
-    if (fail(cudaGraphInstantiate(&exec, graph, 0))) break;
+    if (fail(graphs.events(ev))) break;
+    // the chunk's launches bake in A, the launch shapes and the chunk length
+    const uint64_t topo = topo_signature({prec, chunk, lpg, A.use_sell, gr.a, gr.b, A.use_sell ? sell_grid(A) : 0,
+                                          FEAB_SELL_FUSED_P});
+    auto record = [&](cudaStream_t cs) {
+      for (int c = 0; c < chunk; ++c) {
+        if (prec == FEAB_PREC_FP32) launch_step<FEAB_PREC_FP32>(A, gr, lpg, cs);
+        else if (prec == FEAB_PREC_MIXED) launch_step_sell<FEAB_PREC_MIXED>(A, gr, cs);
+        else if (A.use_sell) launch_step_sell<FEAB_PREC_FP64>(A, gr, cs);
+        else launch_step<FEAB_PREC_FP64>(A, gr, lpg, cs);
+      }
+      cudaMemcpyAsync((void*)flag.ptr, &A.S_->done, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
+    };
+    if (fail(graphs.acquire(&A, sizeof(A), topo, record, &exec))) break;
 
     // Every CG iteration is one step and a reliable step follows at most every iteration, so
     // 2*maxiter + 2 steps always suffice: the host loop is bounded.
@@ -913,11 +902,6 @@ int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, fea
   if (rc == FEAB_OK) {
     if (!fail(cudaMemcpyAsync(&hs, A.S_, sizeof(PcgState), cudaMemcpyDeviceToHost, s))) fail(cudaStreamSynchronize(s));
   }
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
-  if (ev[0]) cudaEventDestroy(ev[0]);
-  if (ev[1]) cudaEventDestroy(ev[1]);
-  if (cs) cudaStreamDestroy(cs);
   if (rc != FEAB_OK) {
     if (result) result->status = rc;
     return rc;
@@ -1143,11 +1127,6 @@ extern "C" int32_t feab_csr_spmv(const feab_csr* M, const feab_sell_operator* se
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-namespace {
-std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[128] = {};  // device address of g_noalloc_scratch, per device ordinal
-}  // namespace
-
 extern "C" size_t feab_pcg_noalloc_scratch_bytes(void) { return kNoAllocScratchBytes; }
 
 extern "C" int32_t feab_pcg_noalloc_max_n(void) {
@@ -1170,20 +1149,12 @@ extern "C" int32_t feab_pcg_solve_noalloc(const feab_csr* M, const double* dinv6
   if (M->group_ptr && M->n_groups <= 0) return FEAB_BAD_ARG;
   if (!(prm->tol >= 0.0)) return FEAB_BAD_ARG;
   if (layout(M->n, FEAB_PREC_FP64, nullptr, nullptr) > kNoAllocScratchBytes) return FEAB_SCRATCH_LIMIT;
-  int dev = 0;
-  FEAB_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 128) return FEAB_BAD_ARG;
+  // The array's device address on the current device, looked up on every call: the lookup
+  // allocates nothing, and a cached address could go stale once the device's context is torn
+  // down and created again (cudaDeviceReset), which moves the array.  The first call on a device
+  // also loads this library's device code there, so it should come before any stream capture.
   void* scratch = nullptr;
-  {
-    // first call on this device: look up the array's device address (with the device current)
-    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-      void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return FEAB_CUDA_ERROR;
-      g_noalloc_ptr[dev] = p;
-    }
-    scratch = g_noalloc_ptr[dev];
-  }
+  if (cudaGetSymbolAddress(&scratch, g_noalloc_scratch) != cudaSuccess || !scratch) return FEAB_CUDA_ERROR;
   PcgArgs A{};
   layout(M->n, FEAB_PREC_FP64, static_cast<char*>(scratch), &A);
   fill_matrix(M, &A);

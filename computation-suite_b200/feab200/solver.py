@@ -18,6 +18,7 @@ Differences, by design:
 """
 from __future__ import annotations
 
+import functools
 import time
 import warnings
 
@@ -97,49 +98,64 @@ class FESystem:
         raise ValueError(f"{who}: unknown DOF name {name!r}; valid names: {list(self.dof_names)}.")
 
     # ------------------------------------------------------------------ input validation
+    # What the reference accepts for node and DOF selections (and the ValueError texts it raises)
+    # is part of the drop-in contract; the checks below are written from that contract:
+    #   * ids come as a scalar, a sequence, an array or a set; float ids are accepted when every
+    #     value is integral; anything else is "must be integers";
+    #   * node selections may instead name mesh node sets (one name or a list of names), which
+    #     select the sorted union of those sets; unknown names are an error;
+    #   * local DOFs may be given by index or by DOF name ("ux", ...);
+    #   * an empty selection and ids outside the valid range are errors.
     @staticmethod
     def _as_int_array(values, what, who):
-        arr = np.asarray(list(values) if isinstance(values, (set, frozenset)) else values).reshape(-1)
-        if arr.size and arr.dtype.kind not in "iu":
-            if arr.dtype.kind == "f" and np.all(arr == np.round(arr)):
-                arr = arr.astype(int)
-            else:
-                raise ValueError(f"{who}: {what} must be integers, got {arr.dtype}.")
-        return arr.astype(int)
+        flat = np.ravel(np.asarray(list(values) if isinstance(values, (set, frozenset)) else values))
+        if flat.size == 0 or np.issubdtype(flat.dtype, np.integer):
+            return flat.astype(np.int64)
+        if np.issubdtype(flat.dtype, np.floating):
+            with np.errstate(invalid="ignore"):
+                ints = flat.astype(np.int64)
+            if np.array_equal(ints.astype(flat.dtype), flat):
+                return ints
+        raise ValueError(f"{who}: {what} must be integers, got {flat.dtype}.")
+
+    @staticmethod
+    def _out_of_range(ids, upper):
+        """Sorted distinct ids outside [0, upper)."""
+        return np.unique(ids[np.logical_or(ids < 0, ids >= upper)]).tolist()
 
     def _check_nodes(self, node_ids, who):
-        if isinstance(node_ids, str) or (isinstance(node_ids, (list, tuple)) and node_ids
-                                         and all(isinstance(n, str) for n in node_ids)):
-            names = [node_ids] if isinstance(node_ids, str) else list(node_ids)
-            sets = getattr(self.mesh, "node_sets", {})
-            missing = [n for n in names if n not in sets]
-            if missing:
-                raise ValueError(f"{who}: unknown node set(s) {missing}; available: {sorted(sets)}.")
-            node_ids = np.unique(np.concatenate([np.asarray(sets[n], dtype=int) for n in names]))
+        set_names = None
+        if isinstance(node_ids, str):
+            set_names = [node_ids]
+        elif isinstance(node_ids, (list, tuple)) and len(node_ids) and all(isinstance(v, str) for v in node_ids):
+            set_names = list(node_ids)
+        if set_names is not None:
+            known = getattr(self.mesh, "node_sets", {})
+            unknown = [nm for nm in set_names if nm not in known]
+            if unknown:
+                raise ValueError(f"{who}: unknown node set(s) {unknown}; available: {sorted(known)}.")
+            node_ids = functools.reduce(np.union1d, [np.asarray(known[nm], dtype=np.int64) for nm in set_names])
         nodes = self._as_int_array(node_ids, "node ids", who)
         if nodes.size == 0:
             raise ValueError(f"{who}: no nodes selected (node_ids is empty).")
         n_nodes = len(self.mesh.nodes)
-        bad = nodes[(nodes < 0) | (nodes >= n_nodes)]
-        if bad.size:
-            raise ValueError(f"{who}: node id(s) {sorted(set(bad.tolist()))[:5]} outside the mesh "
-                             f"(valid range 0..{n_nodes - 1}).")
+        outside = self._out_of_range(nodes, n_nodes)
+        if outside:
+            raise ValueError(f"{who}: node id(s) {outside[:5]} outside the mesh (valid range 0..{n_nodes - 1}).")
         return nodes
 
     def _check_local_dofs(self, dof_indices, who):
-        if isinstance(dof_indices, (set, frozenset)):
-            items = list(dof_indices)
-        elif isinstance(dof_indices, str) or np.ndim(dof_indices) == 0:
-            items = [dof_indices]
+        if isinstance(dof_indices, str) or np.ndim(dof_indices) == 0 and not isinstance(dof_indices, (set, frozenset)):
+            entries = [dof_indices]
         else:
-            items = list(dof_indices)
-        resolved = [self._dof_index_by_name(it, who) if isinstance(it, str) else it for it in items]
-        dofs = self._as_int_array(np.array(resolved), "local DOF indices", who)
+            entries = list(dof_indices)
+        as_index = [self._dof_index_by_name(e, who) if isinstance(e, str) else e for e in entries]
+        dofs = self._as_int_array(np.asarray(as_index), "local DOF indices", who)
         if dofs.size == 0:
             raise ValueError(f"{who}: no DOF indices given.")
-        bad = dofs[(dofs < 0) | (dofs >= self.npn)]
-        if bad.size:
-            raise ValueError(f"{who}: local DOF index {sorted(set(bad.tolist()))} is out of range -- "
+        outside = self._out_of_range(dofs, self.npn)
+        if outside:
+            raise ValueError(f"{who}: local DOF index {outside} is out of range -- "
                              f"Hex8Solid3D has 3 DOF(s) per node, so valid indices are 0..2.")
         return dofs
 

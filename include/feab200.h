@@ -257,12 +257,15 @@ int32_t feab_pcg_solve(const feab_csr* A, const feab_sell_operator* sell, const 
  * cause, or an environment that forbids allocation after start-up.  Same algorithm, arguments
  * and result as feab_pcg_solve with precision FEAB_PREC_FP64, but the workspace is a fixed
  * 32 MiB array in the library's device memory (feab_pcg_noalloc_scratch_bytes), held by every
- * GPU that loads the library until the process exits; n above feab_pcg_noalloc_max_n() (about
- * 838 thousand rows) is rejected with FEAB_SCRATCH_LIMIT before anything is launched.  The
- * function calls no cudaMalloc/cudaFree/cudaHostAlloc and creates no stream, event or graph:
- * it launches the step kernels in chunks and reads the done flag into a stack variable.
- * The first call on a device looks up the array's device address (cudaGetSymbolAddress with
- * that device current); make that first call before any stream capture.  All calls on a device
+ * GPU that loads the library until the process exits; n above feab_pcg_noalloc_max_n() is
+ * rejected with FEAB_SCRATCH_LIMIT before anything is launched.  The limit depends on the SM
+ * count of the device (the per-block partials grow with it): about 838 thousand rows on a
+ * 148-SM B200; query it at run time.  The function calls no cudaMalloc/cudaFree/cudaHostAlloc
+ * and creates no stream, event or graph: it launches the plain CSR step kernels in chunks and
+ * reads the done flag into a stack variable (the allocating entry point's sliced operator and
+ * CUDA graph are faster).  Every call looks up the array's device address on the current device
+ * (cudaGetSymbolAddress; no allocation); the first call on a device also loads the library's
+ * device code there, so make it before any stream capture.  All calls on a device
  * share the one array and it keeps the previous call's contents (each call re-initialises what
  * must start at zero), so calls that overlap on the GPU -- on different streams or threads --
  * race and must be serialised by the caller.  Synchronous. */

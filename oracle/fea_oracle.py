@@ -11,13 +11,15 @@ module.
 """
 from __future__ import annotations
 
+import time
+
 import numpy as np
 import scipy.sparse as sp
 import scipy.sparse.linalg as spla
 
 __all__ = [
     "gauss_legendre", "box_mesh", "perturb_interior", "D_solid3d", "hex8_shape_and_derivs",
-    "hex8_element_stiffness", "hex8_bbar_element_stiffness", "hex8_element_mass", "modal", "global_dofs", "structural_csr", "reduce_free", "fixed_dofs_on_plane",
+    "hex8_element_stiffness", "hex8_bbar_element_stiffness", "hex8_element_mass", "modal", "global_dofs", "structural_csr", "structural_pattern", "reduce_free", "fixed_dofs_on_plane",
     "free_dofs", "quad4_shape_and_derivs", "HEX8_FACES", "facet_load_shares", "facet_mass",
     "jacobi_inverse_diagonal", "preconditioned_cg", "simp_scale", "simp_scale_grad",
     "compliance_sensitivity_closed_form", "pod_singular_values", "element_strain_energy_density",
@@ -240,6 +242,24 @@ def structural_csr(ke, conn, n_dof, dofs_per_node=3):
     return K.tocsr()
 
 
+def structural_pattern(conn, n_dof, free, dofs_per_node=3):
+    """(indptr, indices) of the free x free structural pattern alone: the COO of
+    scatter_global_stiffness (vectorized_assembly.py:217-262, row = repeat(g), col = tile(g))
+    with a one-byte placeholder value, summed by SciPy's COO -> CSR, then
+    K[np.ix_(free, free)] (solver.py:1977-1978).  It is the pattern of
+    reduce_free(structural_csr(...)) without forming the element matrices, for meshes whose
+    FP64 COO would not fit in host memory."""
+    g = global_dofs(conn, dofs_per_node).astype(np.int32)
+    E, m = g.shape
+    row = np.repeat(g, m, axis=1).reshape(-1)
+    col = np.tile(g, (1, m)).reshape(-1)
+    K = sp.coo_matrix((np.ones(row.shape[0], dtype=np.int8), (row, col)), shape=(n_dof, n_dof)).tocsr()
+    del row, col
+    Kff = K[np.ix_(free, free)]
+    Kff.sort_indices()
+    return Kff.indptr, Kff.indices
+
+
 def reduce_free(K, free):
     """Kff = K.tocsr()[np.ix_(free, free)] (solver.py:1977-1978, form_linear_system :1434-1435)."""
     return sp.csr_matrix(K)[np.ix_(free, free)]
@@ -320,12 +340,14 @@ def jacobi_inverse_diagonal(A):
     return 1.0 / d
 
 
-def preconditioned_cg(A, b, d_inv=None, x0=None, tol=1e-8, maxiter=None):
+def preconditioned_cg(A, b, d_inv=None, x0=None, tol=1e-8, maxiter=None, history=None):
     """Hestenes-Stiefel PCG with the reference's exact control flow
     (preconditioned_cg, fea_engine/src/fea_engine/iterative_solvers.py:362-481, SciPy branch
     :434-481): x0 = 0, bnorm = ||b|| (1 if zero), early exit when ||r0||/bnorm < tol,
     LinAlgError when p^T A p <= 0, convergence tested right after the r update, RuntimeError
-    after maxiter = 10 n.  Returns (x, n_iter, final relative residual)."""
+    after maxiter = 10 n.  Returns (x, n_iter, final relative residual).  ``history``, if a
+    list, receives (time.perf_counter(), relative residual) after every iteration, so that one
+    tight solve also gives the time and iterate at any looser tolerance."""
     A = sp.csr_matrix(A)
     b = np.asarray(b, dtype=float)
     n = b.shape[0]
@@ -352,6 +374,8 @@ def preconditioned_cg(A, b, d_inv=None, x0=None, tol=1e-8, maxiter=None):
         x = x + alpha * p
         r = r - alpha * Ap
         rel = np.linalg.norm(r) / bnorm
+        if history is not None:
+            history.append((time.perf_counter(), rel))
         if rel < tol:
             return x, k, rel
         z = Minv(r)

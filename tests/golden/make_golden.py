@@ -2,7 +2,7 @@
 
 Run from the repository root, in a checkout where the reference is available:
 
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <reference checkout>
 
 It imports abhi2k16/computation-suite's ``fea_engine`` and ``rom_engine`` from
 ``<reference>/fea_engine/src`` and ``<reference>/rom_engine/src`` and calls the

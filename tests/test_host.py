@@ -1,4 +1,5 @@
 """Host-side logic (no GPU): mesh numbering, loads, boundary-condition bookkeeping."""
+import os
 import numpy as np
 import pytest
 
@@ -122,3 +123,50 @@ def test_bench_byte_counts():
     """The algorithmic byte formulas the bench's rooflines divide by."""
     import bench
     assert bench.recovery_bytes(10, 4) == 4 * (32 + 448 + 56 + 32 + 32 + 448) + 10 * (48 + 4 + 56)
+
+
+@pytest.mark.parametrize("shape", [(8, 4, 4), (12, 3, 5)])
+def test_oracle_workloads_match_product_workloads(shape):
+    """The oracle's builders (used where the CUDA library must not load: the CPU reference arm and
+    the full-size oracle job) give bit-identical inputs to the product's benchmark problems."""
+    from oracle import workloads as W
+    a, b = W.random_tip_cantilever(*shape), cl.random_tip_cantilever(*shape)
+    for x, y in ((a["nodes"], b.mesh.nodes), (a["elements"], b.mesh.elements), (a["fixed"], b.fixed),
+                 (a["free"], b.free), (a["F"], b.F), (a["D"], b.D)):
+        assert np.array_equal(x, y)
+    a, b = W.simp_cantilever(*shape), cl.simp_cantilever(*shape)
+    assert np.array_equal(a["F"], b.F) and np.array_equal(a["rho"], b.meta["rho"])
+    assert a["load_node"] == b.meta["load_node"] and np.array_equal(a["D"], b.D)
+
+
+def test_oracle_pattern_only_matches_assembled_pattern():
+    nodes, el = O.box_mesh(2.0, 0.4, 0.4, 6, 3, 2)
+    nodes = O.perturb_interior(nodes, (0.3, 0.13, 0.2), 0.1, 3)
+    fixed = O.fixed_dofs_on_plane(nodes)
+    free = O.free_dofs(3 * len(nodes), fixed)
+    K = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(nodes[el], O.D_solid3d(210e9, 0.3)), el,
+                                       3 * len(nodes)), free)
+    ip, ix = O.structural_pattern(el, 3 * len(nodes), free)
+    assert np.array_equal(ip, K.indptr) and np.array_equal(ix, K.indices)
+
+
+def test_reference_arm_runs_whole_steps_without_the_cuda_library():
+    """bench.py --impl reference times whole oracle steps and never imports feab200 (so
+    libfeab200.so is never mapped into that process)."""
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    code = ("import runpy, sys, json; sys.argv = ['bench.py', '--impl', 'reference', '--shape', '8', '2', '2', "
+            "'--steps', '2', '--warmup', '1']; runpy.run_path('bench.py', run_name='__main__'); "
+            "maps = open('/proc/self/maps').read(); "
+            "print(json.dumps({'feab200': any(m.startswith('feab200') for m in sys.modules), "
+            "'so': 'libfeab200' in maps}))")
+    out = subprocess.run([sys.executable, "-c", code], cwd=root, capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [json.loads(ln) for ln in out.stdout.splitlines() if ln.startswith("{")]
+    line, probe = lines[0], lines[1]
+    assert probe == {"feab200": False, "so": False}
+    assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 0
+    assert len(line["step_ms"]) == 2 and line["value"] > 0
+    assert set(line["config"]) == {"workload", "n_free", "nnz", "tol", "l2", "parallelism"}

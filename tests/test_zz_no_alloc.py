@@ -45,17 +45,21 @@ def test_noalloc_pcg_matches_allocating_entry_point(golden):
     from feab200.device import pcg_solve
     g, op = _system(golden)
     b = torch.as_tensor(g["Ff"]).to(op.vals64.device)
-    x_ref, info = pcg_solve(op, b, tol=1e-10, precision="fp64", lanes_per_group=16)
+    # the allocating entry point on the same CSR SpMV kernel, so the iterates agree bit for bit
+    x_ref, info = pcg_solve(op, b, tol=1e-10, precision="fp64", lanes_per_group=16, layout="csr")
     assert info.status == 0
+    u_lu = g["U_lu"][g["free"]]              # the reference's own SuperLU solution
     for _ in range(2):                       # two calls in a row share the fixed scratch
         rc, x, res = _noalloc(op, b, 1e-10)
         assert rc == L.FEAB_OK and res.status == L.FEAB_OK
         assert res.iters == info.iters
         err = float(torch.linalg.norm(x - x_ref) / torch.linalg.norm(x_ref))
         assert err < UTOL, err
+        xh = x.cpu().numpy()
+        assert np.linalg.norm(xh - u_lu) / np.linalg.norm(u_lu) < UTOL
     # a second, different right-hand side: no state leaks from the previous call
     b2 = torch.as_tensor(np.random.default_rng(1).standard_normal(op.n)).to(op.vals64.device)
-    x2_ref, _ = pcg_solve(op, b2, tol=1e-10, precision="fp64", lanes_per_group=16)
+    x2_ref, _ = pcg_solve(op, b2, tol=1e-10, precision="fp64", lanes_per_group=16, layout="csr")
     rc, x2, res = _noalloc(op, b2, 1e-10)
     assert rc == L.FEAB_OK
     assert float(torch.linalg.norm(x2 - x2_ref) / torch.linalg.norm(x2_ref)) < UTOL

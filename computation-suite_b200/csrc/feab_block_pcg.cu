@@ -38,7 +38,15 @@ constexpr int kModeReliable = 1;
 struct ProbState {  // per problem
   int32_t mode, pending, psel, done, status, iters, reliable, last_reliable;
   uint32_t ticket_a, ticket_b;
+  int32_t fp64vals, pad;  // mixed: the problem has switched to the FP64 values (see kFloorFraction)
 };
+
+// Mixed: at an FP64 residual replacement, |r_FP64 - r_recursive| / |b| of a column estimates the
+// residual floor of the 48-bit operator, |(K - K~) x| / |b| (the recursive residual follows the
+// 48-bit operator since the previous replacement).  A problem whose estimate exceeds this fraction
+// of the tolerance cannot reach the tolerance at FP64's iteration count on K~ (it would need an
+// extra refinement cycle), so it continues on the FP64 values from there on.
+constexpr double kFloorFraction = 0.25;
 
 // Mixed: fewest CG steps between two FP64 residual replacements of a problem, unless every
 // unconverged column is ready for one (a replacement is an FP64 SpMM over the whole panel).
@@ -385,6 +393,7 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
         P.iters = 0;
         P.reliable = 0;
         P.last_reliable = 0;
+        P.fp64vals = 0;
         P.status = FEAB_OK;
         P.done = all;
         if (all) atomicSub(A.remaining, 1);
@@ -401,7 +410,9 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
   __shared__ double sm[kWarps][K];
+  __shared__ double smg[MIXED ? kWarps : 1][K];
   __shared__ GroupStage stage[kWarps];
+  __shared__ int switch_vals;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
@@ -409,13 +420,17 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
     const double* __restrict__ po = A.P0;  // the direction, already updated by k_bstep_p
-    double part[CPL];
+    double part[CPL], gap[CPL];
 #pragma unroll
-    for (int q = 0; q < CPL; ++q) part[q] = 0.0;
+    for (int q = 0; q < CPL; ++q) part[q] = gap[q] = 0.0;
     for (int g = A.item_g0[it] + w; g < A.item_g1[it]; g += kWarps) {
       double acc[3][CPL];
-      if (reliable) group_spmm<K, false>(A, g, lane, stage[w], A.X, acc);
-      else group_spmm<K, MIXED>(A, g, lane, stage[w], po, acc);
+      if constexpr (MIXED) {
+        if (reliable || P.fp64vals) group_spmm<K, false>(A, g, lane, stage[w], reliable ? A.X : po, acc);
+        else group_spmm<K, true>(A, g, lane, stage[w], po, acc);
+      } else {
+        group_spmm<K, false>(A, g, lane, stage[w], po, acc);
+      }
       if (lane < LW) {
         const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
 #pragma unroll
@@ -426,8 +441,10 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
             const int64_t idx = (int64_t)(r0 + k) * K + panel_col<K>(lane, q);
             if (reliable) {
               const double ri = A.B[idx] - acc[k][q];
+              const double d = ri - A.R[idx];  // FP64 minus recursive residual
               A.R[idx] = ri;
               part[q] += ri * ri;
+              gap[q] += d * d;
             } else {
               const double pv = po[idx];
               A.AP[idx] = acc[k][q];
@@ -439,23 +456,36 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
     }
     if (lane < LW) {
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) sm[w][panel_col<K>(lane, q)] = part[q];
+      for (int q = 0; q < CPL; ++q) {
+        sm[w][panel_col<K>(lane, q)] = part[q];
+        if constexpr (MIXED) smg[w][panel_col<K>(lane, q)] = gap[q];
+      }
     }
     __syncthreads();
     if (threadIdx.x < K) {
-      double s = 0.0;
-      for (int q = 0; q < kWarps; ++q) s += sm[q][threadIdx.x];
+      double s = 0.0, sg = 0.0;
+      for (int q = 0; q < kWarps; ++q) {
+        s += sm[q][threadIdx.x];
+        if constexpr (MIXED) sg += smg[q][threadIdx.x];
+      }
       A.part[(int64_t)it * 2 * K + threadIdx.x] = s;
+      if (reliable) A.part[(int64_t)it * 2 * K + K + threadIdx.x] = sg;
     }
     const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
     if (last_of_problem(&A.ps[p].ticket_a, n_it)) {
+      if (threadIdx.x == 0) switch_vals = 0;
+      __syncthreads();
       if (threadIdx.x < K) {
         const int c = threadIdx.x;
-        double s = 0.0;
-        for (int q = 0; q < n_it; ++q) s += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
+        double s = 0.0, sg = 0.0;
+        for (int q = 0; q < n_it; ++q) {
+          s += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
+          if (reliable) sg += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + K + c]);
+        }
         ColState& C = A.cs[(int64_t)p * K + c];
         if (reliable) {
           C.rr = s;
+          if (C.active && !C.converged && sqrt(sg) > kFloorFraction * A.tol * C.bnorm) atomicOr(&switch_vals, 1);
         } else {
           C.alpha = 0.0;
           if (C.active && !C.converged) {
@@ -468,6 +498,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
       if (threadIdx.x == 0) {
         ProbState& Pm = A.ps[p];
         Pm.ticket_a = 0;
+        if (switch_vals) Pm.fp64vals = 1;
         if (!reliable) {
           Pm.pending = 0;
           if (Pm.status != FEAB_OK) {
@@ -733,6 +764,36 @@ __global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
   }
 }
 
+// Y = K X for a whole n x K panel (the plain CSR, FP64 values): the SpMM of step A on its own,
+// one warp per node row group, grid-stride over the groups.
+template <int K>
+__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_block_spmm(BArgs A, const double* __restrict__ src,
+                                                                         double* __restrict__ dst) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int LW = K >= 32 ? 32 : K;
+  __shared__ GroupStage stage[kWarps];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  for (int g = blockIdx.x * kWarps + w; g < A.n_groups; g += gridDim.x * kWarps) {
+    double acc[3][CPL];
+    group_spmm<K, false>(A, g, lane, stage[w], src, acc);
+    if (lane < LW) {
+      const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k >= f) break;
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) dst[(int64_t)(r0 + k) * K + panel_col<K>(lane, q)] = acc[k][q];
+      }
+    }
+  }
+}
+
+template <int K>
+void launch_block_spmm(const BArgs& A, const double* X, double* Y, cudaStream_t s) {
+  const int grid = std::max(1, std::min((A.n_groups + kWarps - 1) / kWarps, sm_count() * 8));
+  k_block_spmm<K><<<grid, kThreads, 0, s>>>(A, X, Y);
+}
+
 size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
 
 struct BLayout {
@@ -926,4 +987,32 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
     case 32: return run_block<32>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
     default: return run_block<64>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
   }
+}
+
+extern "C" int32_t feab_block_spmm(const feab_csr* M, const double* X, double* Y, int32_t k, cudaStream_t s) {
+  if (!M || !X || !Y || M->n <= 0 || !M->row_ptr || !M->col_idx || !M->vals64 || !M->group_ptr || M->n_groups <= 0)
+    return FEAB_BAD_ARG;
+  if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64) return FEAB_BAD_ARG;
+  if (X == Y) return FEAB_BAD_ARG;
+  if (k == 64 && ((reinterpret_cast<uintptr_t>(X) & 15) != 0)) return FEAB_BAD_ARG;  // 16-byte panel-row gathers
+  BArgs A{};
+  A.n = M->n;
+  A.n_groups = M->n_groups;
+  A.k = k;
+  A.row_ptr = M->row_ptr;
+  A.col_idx = M->col_idx;
+  A.group_ptr = M->group_ptr;
+  A.vals64 = M->vals64;
+  switch (k) {
+    case 1: launch_block_spmm<1>(A, X, Y, s); break;
+    case 2: launch_block_spmm<2>(A, X, Y, s); break;
+    case 4: launch_block_spmm<4>(A, X, Y, s); break;
+    case 8: launch_block_spmm<8>(A, X, Y, s); break;
+    case 16: launch_block_spmm<16>(A, X, Y, s); break;
+    case 32: launch_block_spmm<32>(A, X, Y, s); break;
+    default: launch_block_spmm<64>(A, X, Y, s); break;
+  }
+  count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
 }

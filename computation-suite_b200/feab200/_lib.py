@@ -105,6 +105,10 @@ SIGNATURES = {
     "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(Batch), _P, _P, _P,
                                     C.POINTER(PcgParams), _P, _SZ, C.POINTER(_I32), C.POINTER(_D), C.POINTER(_I32),
                                     _P]),
+    "feab_block_spmm": (_I32, [C.POINTER(CSR), _P, _P, _I32, _P]),
+    "feab_panel_gram_workspace_bytes": (_SZ, [_I64]),
+    "feab_panel_gram": (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _SZ, _P]),
+    "feab_panel_small": (_I32, [_P, _I32, _I64, _I32, _P, _I32, _P, _I32, _P]),
     "feab_gram_workspace_bytes": (_SZ, [_I64, _I32]),
     "feab_gram_bf16x3": (_I32, [_P, _I64, _I32, _P, _P, _SZ, _P, _P]),
     "feab_gram_fp64": (_I32, [_P, _I32, _I64, _I32, _P, _P, _SZ, _P]),

@@ -14,6 +14,9 @@ K is block diagonal by construction.
 from __future__ import annotations
 
 import ctypes as C
+import json
+import os
+import tempfile
 from dataclasses import dataclass
 
 import numpy as np
@@ -80,19 +83,12 @@ def problem_cost(n_nodes, n_rhs):
     return 3.0 * n_nodes * panel_width(n_rhs)
 
 
-def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=None, precision="fp64",
-              reliable_delta=0.1, chunk=16, max_groups=64):
-    """Solve the panel B_panel (n x K, row-major, device) for the problems whose free rows are
-    [row_bounds[p], row_bounds[p+1]).  Returns (X_panel, BatchResult)."""
-    if precision not in ("fp64", "mixed"):
-        raise ValueError("block PCG precision must be 'fp64' or 'mixed'")
+def _block_pcg_call(op, item_problem, g0, g1, prob_items, B_panel, cols, tol, maxiter, precision, reliable_delta,
+                    chunk):
+    """One feab_block_pcg_solve over a panel of width B_panel.shape[1] (a power of two)."""
     dev = op.vals64.device
     n, K = B_panel.shape
-    if n != op.n or K not in PANELS:
-        raise ValueError(f"panel must be ({op.n}, k) with k in {PANELS}")
-    gp = op.pattern.group_ptr.cpu().numpy()
-    item_problem, g0, g1, prob_items = _work_items(gp, np.asarray(row_bounds), max_groups)
-    P = len(row_bounds) - 1
+    P = len(prob_items) - 1
     t = lambda a: torch.as_tensor(a).to(dev)  # noqa: E731
     ip, ig0, ig1, pit, pcols = t(item_problem), t(g0), t(g1), t(prob_items), t(np.asarray(cols, np.int32))
     batch = L.Batch(P, K, len(item_problem), 0, ip.data_ptr(), ig0.data_ptr(), ig1.data_ptr(), pit.data_ptr(),
@@ -116,6 +112,162 @@ def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=
     if rc in (L.FEAB_BAD_ARG, L.FEAB_CUDA_ERROR):
         L.raise_for(rc, "block PCG")
     return X, BatchResult(status, iters.reshape(P, K), relres.reshape(P, K))
+
+
+def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=None, precision="fp64",
+              reliable_delta=0.1, chunk=16, max_groups=None, tile_width=None, tune=True):
+    """Solve the panel B_panel (n x K, row-major, device) for the problems whose free rows are
+    [row_bounds[p], row_bounds[p+1]).  Returns (X_panel, BatchResult).
+
+    Launch shape: work items of ``max_groups`` node row groups, and the panel processed in
+    column tiles of ``tile_width`` (each tile is its own block solve; K is streamed once per
+    tile and step).  Left as None they come from ``tuned_block_shape`` (timed once per
+    operator shape and cached) when ``tune`` is true, else 64 groups and the full width."""
+    if precision not in ("fp64", "mixed"):
+        raise ValueError("block PCG precision must be 'fp64' or 'mixed'")
+    n, K = B_panel.shape
+    if n != op.n or K not in PANELS:
+        raise ValueError(f"panel must be ({op.n}, k) with k in {PANELS}")
+    cols = np.asarray(cols, np.int64)
+    if max_groups is None or tile_width is None:
+        if tune:
+            shape = tuned_block_shape(op, row_bounds, B_panel, cols, precision)
+        else:
+            shape = BlockShape(64, K, None)
+        max_groups = shape.item_groups if max_groups is None else max_groups
+        tile_width = shape.tile_width if tile_width is None else tile_width
+    if tile_width not in PANELS or tile_width > K:
+        raise ValueError(f"tile_width must be a panel width <= {K}, got {tile_width}")
+    if int(max_groups) < 1:
+        raise ValueError("max_groups must be >= 1")
+    gp = op.pattern.group_ptr.cpu().numpy()
+    items = _work_items(gp, np.asarray(row_bounds), int(max_groups))
+    if tile_width == K:
+        return _block_pcg_call(op, *items, B_panel, cols, tol, maxiter, precision, reliable_delta, chunk)
+    P = len(row_bounds) - 1
+    X = torch.zeros((n, K), dtype=torch.float64, device=op.vals64.device)
+    status = np.zeros(P, np.int32)
+    iters = np.zeros((P, K), np.int32)
+    relres = np.zeros((P, K), np.float64)
+    for c0 in range(0, K, tile_width):
+        ct = np.clip(cols - c0, 0, tile_width)
+        if not ct.any():
+            continue
+        Xt, rt = _block_pcg_call(op, *items, B_panel[:, c0:c0 + tile_width], ct, tol, maxiter, precision,
+                                 reliable_delta, chunk)
+        X[:, c0:c0 + tile_width] = Xt
+        iters[:, c0:c0 + tile_width] = rt.iters
+        relres[:, c0:c0 + tile_width] = rt.relres
+        status = np.where(status == 0, rt.status, status)
+    return X, BatchResult(status, iters, relres)
+
+
+# ----------------------------------------------------------------------------- launch-shape tuner
+ITEM_GROUPS = (16, 32, 64, 128)
+
+
+@dataclass
+class BlockShape:
+    item_groups: int          # node row groups per work item (the "elements per block" of the SpMM)
+    tile_width: int           # right-hand-side columns per block solve
+    us_per_step: float | None  # measured cost of one block-PCG step of the whole panel
+
+
+_tuned_block = {}
+
+
+def tuning_cache_path():
+    """JSON file of tuned block-PCG launch shapes: $FEAB_TUNING_CACHE, else
+    ~/.cache/feab200/block_pcg_tuning.json."""
+    return os.environ.get("FEAB_TUNING_CACHE") or os.path.join(os.path.expanduser("~"), ".cache", "feab200",
+                                                               "block_pcg_tuning.json")
+
+
+def tuning_key(device_name, n, nnz, n_problems, k, precision):
+    return f"{device_name}|n={n}|nnz={nnz}|problems={n_problems}|k={k}|{precision}"
+
+
+def load_tuning(path=None):
+    path = path or tuning_cache_path()
+    try:
+        with open(path) as fh:
+            raw = json.load(fh)
+    except (OSError, ValueError):
+        return {}
+    out = {}
+    for key, v in raw.items() if isinstance(raw, dict) else ():
+        try:
+            shape = BlockShape(int(v["item_groups"]), int(v["tile_width"]),
+                               None if v.get("us_per_step") is None else float(v["us_per_step"]))
+        except (KeyError, TypeError, ValueError):
+            continue
+        if shape.item_groups >= 1 and shape.tile_width in PANELS:
+            out[key] = shape
+    return out
+
+
+def save_tuning(key, shape, path=None):
+    """Merge one entry into the cache file (written to a temporary file and renamed, so a
+    concurrent reader never sees a partial file)."""
+    path = path or tuning_cache_path()
+    entries = {k: {"item_groups": s.item_groups, "tile_width": s.tile_width, "us_per_step": s.us_per_step}
+               for k, s in load_tuning(path).items()}
+    entries[key] = {"item_groups": shape.item_groups, "tile_width": shape.tile_width, "us_per_step": shape.us_per_step}
+    try:
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        fd, tmp = tempfile.mkstemp(dir=os.path.dirname(path) or ".", suffix=".tmp")
+        with os.fdopen(fd, "w") as fh:
+            json.dump(entries, fh, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass                   # a read-only home directory keeps the in-process cache only
+
+
+def _step_cost_us(op, items, B_panel, cols, precision, short=4, long=20):
+    """Device time of one block-PCG step over this panel: two runs of tol 0 (no column
+    converges) of `short` and `long` steps, timed with CUDA events; the difference over
+    long - short removes setup and graph capture."""
+    times = []
+    for steps in (short, long, short, long):
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        _block_pcg_call(op, *items, B_panel, cols, 0.0, steps, precision, 0.1, 8)
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b) * 1e3)
+    return max(1e-3, (min(times[1], times[3]) - min(times[0], times[2])) / (long - short))
+
+
+def tuned_block_shape(op, row_bounds, B_panel, cols, precision="fp64", candidates=None):
+    """The (work-item groups, column tile width) with the cheapest measured block-PCG step for
+    this operator and panel, timed on the actual operator and right-hand sides over
+    ITEM_GROUPS x {panel widths <= K}; a tile narrower than K costs K / width tile steps.
+    Cached in this process and in the JSON file of tuning_cache_path(), keyed by (GPU, n, nnz,
+    problems, K, precision)."""
+    n, K = B_panel.shape
+    P = len(row_bounds) - 1
+    dev = op.vals64.device
+    key = tuning_key(torch.cuda.get_device_name(dev), op.n, op.nnz, P, K, precision)
+    hit = _tuned_block.get(key)
+    if hit is None:
+        hit = load_tuning().get(key)
+    if hit is not None:
+        _tuned_block[key] = hit
+        return hit
+    gp = op.pattern.group_ptr.cpu().numpy()
+    cols = np.asarray(cols, np.int64)
+    if candidates is None:
+        candidates = [(g, w) for g in ITEM_GROUPS for w in PANELS if 16 <= w <= K or w == K]
+    best = None
+    for g, w in candidates:
+        items = _work_items(gp, np.asarray(row_bounds), g)
+        ct = np.clip(cols, 0, w)
+        cost = _step_cost_us(op, items, B_panel[:, :w].contiguous(), ct, precision) * (K // w)
+        if best is None or cost < best.us_per_step:
+            best = BlockShape(g, w, cost)
+    _tuned_block[key] = best
+    save_tuning(key, best)
+    return best
 
 
 class ProblemBatch:

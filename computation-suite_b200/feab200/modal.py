@@ -5,11 +5,12 @@ Lanczos on a sparse LU factorisation.  feab200 finds the same lowest eigenpairs 
 K phi = lambda M phi by block subspace iteration (inverse iteration on a block of p > n_modes
 vectors) with a Rayleigh-Ritz step, every product on the GPU:
 
-    Y  = K^-1 (M X)                 block-PCG, one column per vector (feab_block_pcg_solve)
-    Kr = Y^T K Y,  Mr = Y^T M Y      CSR SpMVs (feab_csr_spmv) and FP64 cuBLAS GEMMs
+    Y  = K^-1 (M X)                 block-PCG over the block of vectors (feab_block_pcg_solve),
+                                     M X by the block SpMM (feab_block_spmm)
+    Kr = Y^T K Y,  Mr = Y^T M Y      block SpMMs and FP64 panel Grams (feab_panel_gram)
     Kr v = lambda Mr v               Mr = Q L Q^T, then the eigenpairs of L^-1/2 Q^T Kr Q L^-1/2
-                                     (feab_symeig_jacobi, one CTA, k <= 64)
-    X  = Y V                         M-orthonormal Ritz vectors, lambda ascending
+                                     (feab_symeig_jacobi, one CTA, k <= 64; p x p products only)
+    X  = Y V                         M-orthonormal Ritz vectors, lambda ascending (feab_panel_small)
 
 until the n_modes lowest Ritz values change by less than ``tol`` (relative).  Ritz values converge
 like (lambda_i / lambda_{p+1})^(2j), so the block is wider than the number of modes asked for.
@@ -20,17 +21,9 @@ import numpy as np
 import torch
 
 from .batched import block_pcg, panel_width
-from .device import ReducedOperator, spmv
+from .device import ReducedOperator
+from .panel import block_spmm, panel_gram, panel_small
 from .pod import symeig
-
-
-def _apply_columns(op: ReducedOperator, X):
-    """op @ X for an (n, p) device panel, one CSR SpMV per column."""
-    XT = X.t().contiguous()
-    out = torch.empty_like(XT)
-    for j in range(XT.shape[0]):
-        spmv(op, XT[j], "fp64", out=out[j])
-    return out.t()
 
 
 def _generalized_eig(Kr, Mr):
@@ -59,19 +52,23 @@ def subspace_iteration(Kop: ReducedOperator, Mop: ReducedOperator, n_modes, subs
     K = panel_width(p)
     dev = Kop.vals64.device
     g = torch.Generator(device=dev).manual_seed(int(seed))
-    X = torch.randn((n, p), generator=g, dtype=torch.float64, device=dev)
-    B = torch.zeros((n, K), dtype=torch.float64, device=dev)
+    X = torch.zeros((n, K), dtype=torch.float64, device=dev)      # panel of width K, columns >= p zero
+    X[:, :p] = torch.randn((n, p), generator=g, dtype=torch.float64, device=dev)
+    B = torch.empty((n, K), dtype=torch.float64, device=dev)
+    KY = torch.empty_like(B)
+    MY = torch.empty_like(B)
     lam_old = None
     for it in range(1, maxiter + 1):
-        B[:, :p] = _apply_columns(Mop, X)
+        block_spmm(Mop, X, out=B)
         Y, res = block_pcg(Kop, np.array([0, n]), B, [p], tol=pcg_tol)
         if not (res.status == 0).all():
             raise RuntimeError(f"solve_modal: the inner block-PCG did not converge (status {res.status.tolist()})")
-        Y = Y[:, :p]
-        Kr = Y.t() @ _apply_columns(Kop, Y)
-        Mr = Y.t() @ _apply_columns(Mop, Y)
+        block_spmm(Kop, Y, out=KY)
+        block_spmm(Mop, Y, out=MY)
+        Kr = panel_gram(Y[:, :p], KY[:, :p])
+        Mr = panel_gram(Y[:, :p], MY[:, :p])
         lam, V = _generalized_eig(0.5 * (Kr + Kr.t()), 0.5 * (Mr + Mr.t()))
-        X = Y @ V
+        X[:, :p] = panel_small(Y[:, :p], V)
         low = lam[:n_modes]
         if lam_old is not None:
             change = float(((low - lam_old).abs() / low.abs().clamp_min(1e-300)).max())

@@ -22,6 +22,7 @@ import torch
 
 from . import _lib as L
 from .device import cuda_device
+from .panel import panel_small
 
 MAX_SNAPSHOTS = 64
 
@@ -128,7 +129,8 @@ class PodBasis:
         r = _select_rank(S_host, n_modes, energy_threshold)
         Vk = V[:k, :r]                                       # eigenvectors of the k x k Gram block
         inv = torch.where(S[:r] > 0, 1.0 / S[:r], torch.zeros_like(S[:r]))
-        self.V = (X.to(torch.float64) @ Vk) * inv[None, :]   # method of snapshots: U = X V / sigma
+        # method of snapshots: U = X V / sigma, as one panel product (V scaled by 1 / sigma first)
+        self.V = panel_small(X.to(torch.float64), (Vk * inv[None, :]).contiguous())
         self.singular_values = S_host
         self.n_modes = r
         return self

@@ -326,6 +326,12 @@ int32_t feab_block_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, 
                              void* workspace, size_t workspace_bytes, int32_t* iters_out, double* relres_out,
                              int32_t* status_out, cudaStream_t stream);
 
+/* Y = A X for a row-major n x k panel X (k in {1,2,4,8,16,32,64}; X 16-byte aligned for
+ * k = 64): the block-PCG's SpMM on the plain CSR (FP64 values, node row groups required) on its
+ * own.  Applies K_ff or M_ff to the whole block of vectors of the modal subspace iteration (the
+ * products eigsh makes inside FESystem.solve_modal, solver.py:2047-2114).  Asynchronous. */
+int32_t feab_block_spmm(const feab_csr* A, const double* X, double* Y, int32_t k, cudaStream_t stream);
+
 /* ---------------------------------------------------------------- POD Gram + eigensolve
  * Replaces the FP64 economy SVD of PodBasis._fit_standard (rom_engine/src/rom_engine/pod.py:
  * 140-147) for the singular values: G = X^T X with X (n x 64, FP32, row major, 16-byte
@@ -345,6 +351,22 @@ int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double* G, void* 
  * gets such trailing singular values right).  Asynchronous on the stream; deterministic. */
 int32_t feab_gram_fp64(const void* X, int32_t x_bytes, int64_t n, int32_t k, double* G, void* workspace,
                        size_t workspace_bytes, cudaStream_t stream);
+
+/* C = X^T Y (k x k, row major, FP64) for row-major n x k FP64 panels X and Y with leading
+ * dimensions ldx, ldy (k <= 64): the Rayleigh-Ritz projections Y^T K Y and Y^T M Y of the modal
+ * subspace iteration (the dense products behind eigsh in FESystem.solve_modal, solver.py:
+ * 2047-2114).  Per-CTA partials in the workspace (feab_panel_gram_workspace_bytes(n)) are summed
+ * in a fixed order, so C is deterministic.  Asynchronous. */
+size_t feab_panel_gram_workspace_bytes(int64_t n);
+int32_t feab_panel_gram(const double* X, int32_t ldx, const double* Y, int32_t ldy, int64_t n, int32_t k, double* C,
+                        void* workspace, size_t workspace_bytes, cudaStream_t stream);
+
+/* Z = Y V for a row-major n x k FP64 panel Y (leading dimension ldy, k <= 64) and a row-major
+ * k x m matrix V (m <= 64), into the n x m panel Z (leading dimension ldz; Z must not be Y):
+ * the Ritz vectors of the modal subspace iteration and the POD modes X V / sigma
+ * (rom_engine/src/rom_engine/pod.py:140-160).  Asynchronous. */
+int32_t feab_panel_small(const double* Y, int32_t ldy, int64_t n, int32_t k, const double* V, int32_t m, double* Z,
+                         int32_t ldz, cudaStream_t stream);
 
 /* Cyclic Jacobi eigensolver (one CTA, FP64) for a symmetric k x k matrix (k <= 64) in device
  * memory: eigenvalues descending into evals, eigenvectors (columns) into evecs (may be NULL).

@@ -170,3 +170,25 @@ def test_reference_arm_runs_whole_steps_without_the_cuda_library():
     assert line["impl"] == "reference" and line["steps"] == 2 and line["warmup"] == 0
     assert len(line["step_ms"]) == 2 and line["value"] > 0
     assert set(line["config"]) == {"workload", "n_free", "nnz", "tol", "l2", "parallelism"}
+
+
+def test_block_tuning_cache_round_trip(tmp_path):
+    from feab200 import batched as bt
+    path = str(tmp_path / "sub" / "tuning.json")
+    k1 = bt.tuning_key("NVIDIA B200", 418176, 32348142, 1, 64, "fp64")
+    k2 = bt.tuning_key("NVIDIA B200", 418176, 32348142, 1, 64, "mixed")
+    assert k1 != k2
+    bt.save_tuning(k1, bt.BlockShape(32, 64, 512.5), path)
+    bt.save_tuning(k2, bt.BlockShape(128, 32, 480.0), path)
+    got = bt.load_tuning(path)
+    assert got == {k1: bt.BlockShape(32, 64, 512.5), k2: bt.BlockShape(128, 32, 480.0)}
+    # malformed entries are ignored, a missing or corrupt file reads as empty
+    import json
+    raw = json.load(open(path))
+    raw["bad"] = {"item_groups": 0, "tile_width": 64}
+    raw["worse"] = {"tile_width": 3}
+    json.dump(raw, open(path, "w"))
+    assert set(bt.load_tuning(path)) == {k1, k2}
+    open(path, "w").write("{not json")
+    assert bt.load_tuning(path) == {}
+    assert bt.load_tuning(str(tmp_path / "missing.json")) == {}

@@ -571,8 +571,11 @@ __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
 
 // Step B: X += alpha P, R -= alpha AP (CG step; a reliable step leaves both); per column r.r
 // and r.z with z = M r formed on the fly; per-column convergence, beta, problem bookkeeping.
+#ifndef FEAB_BLOCK_B_MINB
+#define FEAB_BLOCK_B_MINB 1
+#endif
 template <int K, bool MIXED>
-__global__ void __launch_bounds__(kThreads) k_bstep_b(BArgs A) {
+__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A) {
   __shared__ double sm[2][kThreads];
   __shared__ double smv[2][2 * kThreads];
   __shared__ int flag_any, flag_all;

@@ -282,6 +282,276 @@ __global__ void __launch_bounds__(kThreadsG) k_gram_bf16x3(const float* __restri
   for (int j = 0; j < kCols; ++j) out[j] = acc[j];
 }
 
+// ---------------------------------------------------------------- exact-product int8 Gram
+// G = X^T X with the products formed exactly on the tensor cores (tcgen05.mma kind::i8, s32
+// accumulation), after the integer-slice method of Ozaki et al. for emulating high-precision
+// products on integer matrix units (Ootomo, Ozaki & Yokota, "DGEMM on integer matrix
+// multiplication unit", Int. J. High Perf. Comput. Appl. 2024).  Each CTA owns a contiguous range
+// of rows.  Per column i it takes e_i with |x| < 2^e_i over its rows, and splits every value into
+// kSlices signed 7-bit digits: x = 2^e_i sum_a s_a 2^(-7a), s_a = trunc of the scaled remainder
+// (all steps exact in FP32).  Then
+//   x_ri x_rj = 2^(e_i + e_j) sum_{a, c} s_a(r, i) s_c(r, j) 2^(-7(a + c)),
+// and the digit products sum exactly in int32.  Pairs with a + c > kSlices + 1 are dropped
+// (their weight is below 2^(-7(kSlices + 2)) of the scale).  With 7 digits a value keeps 49 bits
+// below its CTA's column maximum, so the FP32 inputs are exact down to 2^-25 of that maximum and
+// the dropped terms are below 1e-15 of it: G comes out with FP64-level accuracy.
+//
+// MMA arrangement (M = 128, N = 64, K = 64 per chunk of 64 rows): A = [S_a ; S_(a+1)] for odd a
+// (S_8 = 0), B = S_c; the product adds S_a^T S_c (weight a + c) to the top 64 TMEM lanes and
+// S_(a+1)^T S_c (weight a + c + 1) to the bottom 64 of region R_(a+c).  Seven regions
+// R_2..R_8 of 64 columns each (448 of TMEM's 512) hold every needed pair with a fixed weight
+// per half: weight v on top of R_v, v + 1 on the bottom.  16 MMAs (32 instructions) per chunk.
+// The int32 regions are drained into FP64 registers every kI8Drain chunks (and at the end),
+// which bounds them below 2^31.  Per-CTA FP64 partials are summed by k_gram_reduce (fixed order).
+constexpr int kSlices = 7;
+constexpr int kI8Threads = 256;
+constexpr int kI8Drain = 192;                        // chunks between drains: < 2^31 / (4 * 64 * 127^2)
+constexpr uint32_t kI8LBO = 128;                     // next core matrix (16 K-bytes) along K
+constexpr uint32_t kI8SBO = 4 * 128;                 // next 8-row group along M / N
+constexpr int kI8SliceBytes = 64 * kChunk;           // one 64-row x 64-K int8 slice tile
+constexpr int kI8Regions = kSlices;                  // R_2 .. R_8
+
+struct __align__(1024) Int8Smem {
+  float stage[kStages][kChunk * kCols];              // 64 KB; reused for the final row exchange
+  int8_t tile[2][(kSlices + 1) * kI8SliceBytes];     // 2 x 32 KB; slice 8 stays zero
+  unsigned long long full_bar[kStages];
+  unsigned long long mma_bar[2];
+  float colmax[kI8Threads / 16][kCols];
+  int expo[kCols];
+  uint32_t tmem_base;
+};
+
+__device__ __forceinline__ uint64_t smem_desc_i8(uint32_t addr) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((kI8LBO >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((kI8SBO >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;
+  return d;
+}
+
+// kind::i8 instruction descriptor: s32 accumulate (D format 2), signed 8-bit A and B, both
+// K-major, N = 64, M = 128.
+__host__ __device__ constexpr uint32_t instr_desc_i8() {
+  return (2u << 4) | (1u << 7) | (1u << 10) | ((64u >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t accum) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(idesc), "r"(accum)
+      : "memory");
+}
+
+// Split the staged FP32 rows of one chunk into the kSlices int8 digit tiles.  Thread t owns
+// column m = t % 64 and rows 16 (t / 64) .. +15 (one 16-byte core-matrix row per digit).
+__device__ __forceinline__ void split_chunk_i8(const float* st, int8_t* tiles, int rows, const int* expo) {
+  const int m = threadIdx.x & 63, kg = threadIdx.x >> 6;
+  const int e = expo[m];
+  int32_t packed[kSlices][4];
+#pragma unroll
+  for (int a = 0; a < kSlices; ++a)
+#pragma unroll
+    for (int w = 0; w < 4; ++w) packed[a][w] = 0;
+#pragma unroll
+  for (int u = 0; u < 16; ++u) {
+    const int k = kg * 16 + u;
+    float y = k < rows ? ldexpf(st[k * kCols + m], 7 - e) : 0.0f;  // |y| < 128
+#pragma unroll
+    for (int a = 0; a < kSlices; ++a) {
+      const float d = truncf(y);
+      y = (y - d) * 128.0f;
+      packed[a][u >> 2] |= (int32_t)(((uint32_t)(int32_t)d & 0xffu) << (8 * (u & 3)));
+    }
+  }
+  const uint32_t off = (m / 8) * kI8SBO + kg * kI8LBO + (m % 8) * 16;
+#pragma unroll
+  for (int a = 0; a < kSlices; ++a)
+    *reinterpret_cast<int4*>(tiles + a * kI8SliceBytes + off) =
+        make_int4(packed[a][0], packed[a][1], packed[a][2], packed[a][3]);
+}
+
+__global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __restrict__ X, int64_t n,
+                                                            double* __restrict__ part, int* err) {
+  extern __shared__ unsigned char smem_raw[];
+  Int8Smem& S = *reinterpret_cast<Int8Smem*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int64_t n_chunks = (n + kChunk - 1) / kChunk;
+  const int64_t per = (n_chunks + gridDim.x - 1) / gridDim.x;
+  const int64_t c0 = min64(n_chunks, (int64_t)blockIdx.x * per), c1 = min64(n_chunks, c0 + per);
+  const int64_t my = c1 - c0;
+  const int64_t row0 = c0 * kChunk, row1 = min64(n, c1 * kChunk);
+
+  // per-column exponents over this CTA's rows: thread t reads 4 columns (float4) of rows
+  // row0 + t / 16, + 16, ...
+  {
+    float mx[4] = {0.f, 0.f, 0.f, 0.f};
+    const int cq = (tid & 15) * 4;
+    for (int64_t r = row0 + (tid >> 4); r < row1; r += kI8Threads / 16) {
+      const float4 v = __ldg(reinterpret_cast<const float4*>(X + r * kCols + cq));
+      mx[0] = fmaxf(mx[0], fabsf(v.x));
+      mx[1] = fmaxf(mx[1], fabsf(v.y));
+      mx[2] = fmaxf(mx[2], fabsf(v.z));
+      mx[3] = fmaxf(mx[3], fabsf(v.w));
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) S.colmax[tid >> 4][cq + j] = mx[j];
+  }
+  // zero both tile buffers (the eighth digit tile must stay zero)
+  for (int i = tid; i < 2 * (kSlices + 1) * kI8SliceBytes / 16; i += kI8Threads)
+    reinterpret_cast<int4*>(&S.tile[0][0])[i] = make_int4(0, 0, 0, 0);
+  if (tid == 0) {
+    for (int s = 0; s < kStages; ++s) mbar_init(&S.full_bar[s], 1);
+    mbar_init(&S.mma_bar[0], 1);
+    mbar_init(&S.mma_bar[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&S.tmem_base)),
+                 "r"(512)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (tid < kCols) {
+    float m = 0.f;
+    for (int g = 0; g < kI8Threads / 16; ++g) m = fmaxf(m, S.colmax[g][tid]);
+    int e = 0;
+    if (m > 0.f) frexpf(m, &e);  // m = f 2^e, f in [0.5, 1): every |x| <= m < 2^e
+    S.expo[tid] = e;
+  }
+  __syncthreads();
+  const uint32_t tmem = S.tmem_base;
+  const uint32_t idesc = instr_desc_i8();
+
+  if (tid == 0) {
+    for (int64_t i = 0; i < min64(my, kStages); ++i) {
+      const int64_t r0 = (c0 + i) * kChunk;
+      const int rows = (int)min64(kChunk, n - r0);
+      bulk_load(S.stage[i], X + r0 * kCols, (uint32_t)rows * kCols * 4, &S.full_bar[i]);
+    }
+  }
+
+  // thread t drains TMEM lane 32 (warp % 4) + lane, regions [rbeg, rend): warps 0-3 take
+  // R_2..R_5, warps 4-7 R_6..R_8
+  const int lane_row = 32 * (warp & 3) + lane;
+  const int rbeg = warp < 4 ? 0 : 4, rend = warp < 4 ? 4 : kI8Regions;
+  double acc[kCols];
+#pragma unroll
+  for (int j = 0; j < kCols; ++j) acc[j] = 0.0;
+  bool ok = true;
+  int since_drain = 0;
+  int64_t issued = 0;
+  uint32_t seen = 0;  // regions written since the last drain (thread 0)
+
+  auto drain = [&](int64_t last) {
+    const bool w = mbar_wait(&S.mma_bar[last & 1], (uint32_t)((last >> 1) & 1), err);
+    if (!__syncthreads_and(w)) {
+      ok = false;
+      return;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
+    // top lanes hold weight v of R_v, bottom lanes weight v + 1
+    const int wshift = lane_row < 64 ? 0 : 1;
+    for (int r = rbeg; r < rend; ++r) {
+      const double scale = ldexp(1.0, -7 * (r + 2 + wshift));
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        float v[32];
+        tmem_ld32(tmem + lane_base + (uint32_t)(r * 64 + h * 32), v);
+#pragma unroll
+        for (int i = 0; i < 32; ++i) acc[h * 32 + i] += (double)__float_as_int(v[i]) * scale;
+      }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  };
+
+  for (int64_t i = 0; i < my && ok; ++i) {
+    const int s = (int)(i % kStages), t = (int)(i & 1);
+    const int rows = (int)min64(kChunk, n - (c0 + i) * kChunk);
+    bool w = true;
+    if (i >= 2 && since_drain > 0) w = mbar_wait(&S.mma_bar[t], (uint32_t)(((i - 2) >> 1) & 1), err);
+    if (w) w = mbar_wait(&S.full_bar[s], (uint32_t)((i / kStages) & 1), err);
+    if (!__syncthreads_and(w)) {
+      ok = false;
+      break;
+    }
+    split_chunk_i8(S.stage[s], S.tile[t], rows, S.expo);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+    if (tid == 0 && i + kStages < my) {
+      const int64_t r2 = (c0 + i + kStages) * kChunk;
+      const int rows2 = (int)min64(kChunk, n - r2);
+      bulk_load(S.stage[s], X + r2 * kCols, (uint32_t)rows2 * kCols * 4, &S.full_bar[s]);
+    }
+    if (tid == 0) {
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const uint32_t base = smem_u32(S.tile[t]);
+      for (int a = 1; a <= kSlices; a += 2) {
+        for (int c = 1; c + a <= kSlices + 1; ++c) {
+          const int v = a + c;  // region R_v, TMEM columns (v - 2) * 64
+#pragma unroll
+          for (int ks = 0; ks < kChunk / 32; ++ks) {
+            const uint64_t da = smem_desc_i8(base + (a - 1) * kI8SliceBytes + ks * 2 * kI8LBO);
+            const uint64_t db = smem_desc_i8(base + (c - 1) * kI8SliceBytes + ks * 2 * kI8LBO);
+            mma_i8(tmem + (uint32_t)((v - 2) * 64), da, db, idesc, ((seen >> v) & 1u) || ks > 0 ? 1u : 0u);
+          }
+          seen |= 1u << v;
+        }
+      }
+      mma_commit(&S.mma_bar[t]);
+    }
+    ++issued;
+    ++since_drain;
+    if (since_drain == kI8Drain || i + 1 == my) {
+      drain(i);
+      since_drain = 0;
+      seen = 0;
+      __syncthreads();
+      if (!ok) break;
+    }
+  }
+  if (!ok) {
+    // bounded waits for what is still in flight before TMEM and shared memory are left: the
+    // MMAs of the last issued chunk and the bulk copies of chunks issued - 1 + 1 .. loaded - 1
+    const long long t0 = clock64();
+    if (issued > 0) {
+      const int64_t last = issued - 1;
+      while (!mbar_try(&S.mma_bar[last & 1], (uint32_t)((last >> 1) & 1)) && clock64() - t0 < kWaitCycles) {
+      }
+    }
+    const int64_t loaded = min64(my, issued + kStages);
+    for (int64_t j = issued; j < loaded; ++j)
+      while (!mbar_try(&S.full_bar[j % kStages], (uint32_t)((j / kStages) & 1)) && clock64() - t0 < 2 * kWaitCycles) {
+      }
+  }
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
+  }
+  // warps 4-7 hand their sums to warps 0-3 (same TMEM rows) through the staging area, then the
+  // partial row lane_row (top: column lane_row of X, bottom: column lane_row - 64), scaled by
+  // 2^(e_i + e_j), goes to part[cta][lane_row][j]
+  double* xch = reinterpret_cast<double*>(&S.stage[0][0]);  // 128 x 64 doubles = 64 KB
+  if (warp >= 4) {
+#pragma unroll
+    for (int j = 0; j < kCols; ++j) xch[lane_row * kCols + j] = acc[j];
+  }
+  __syncthreads();
+  if (warp < 4) {
+    const int ci = lane_row & 63;
+    const int ei = S.expo[ci];
+    double* out = part + ((int64_t)blockIdx.x * 128 + lane_row) * kCols;
+#pragma unroll
+    for (int j = 0; j < kCols; ++j) out[j] = ldexp(acc[j] + xch[lane_row * kCols + j], ei + S.expo[j]);
+  }
+}
+
 // G[m][n] = sum over CTAs of part[cta][m][n] + part[cta][64+m][n]; then symmetrised.  One warp
 // per entry: lane l sums CTAs l, l+32, ... in order, then a fixed shuffle tree (deterministic).
 constexpr int kReduceWarps = 8;
@@ -551,6 +821,24 @@ extern "C" int32_t feab_symeig_jacobi(double* A, int32_t k, double* evals, doubl
   FEAB_CUDA(cudaFuncSetAttribute(k_symeig_jacobi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_symeig_jacobi<<<1, 256, smem, s>>>(A, k, evals, evecs, max_sweeps > 0 ? max_sweeps : 40, sweeps_out);
   count_launches(1);
+  FEAB_CHECK_LAUNCH();
+  return FEAB_OK;
+}
+
+extern "C" int32_t feab_gram_int8(const float* X, int64_t n, int32_t k, double* G, void* workspace,
+                                  size_t workspace_bytes, int32_t* error_flag, cudaStream_t s) {
+  if (!X || !G || !workspace || !error_flag || n <= 0 || k != kCols) return FEAB_BAD_ARG;
+  if ((reinterpret_cast<uintptr_t>(X) & 15) != 0) return FEAB_BAD_ARG;  // bulk copies and float4 reads
+  if (feab_gram_workspace_bytes(n, k) > workspace_bytes) return FEAB_BAD_ARG;
+  const int64_t chunks = (n + kChunk - 1) / kChunk;
+  // contiguous row ranges, one CTA per SM; each CTA's chunk count bounds the int32 drains
+  const int grid = (int)std::max<int64_t>(1, std::min<int64_t>(chunks, (int64_t)sm_count()));
+  const size_t smem = sizeof(Int8Smem) + 1024;
+  FEAB_CUDA(cudaFuncSetAttribute(k_gram_int8, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  double* part = static_cast<double*>(workspace);
+  k_gram_int8<<<grid, kI8Threads, smem, s>>>(X, n, part, error_flag);
+  k_gram_reduce<<<(kCols * kCols + kReduceWarps - 1) / kReduceWarps, 32 * kReduceWarps, 0, s>>>(part, grid, G);
+  count_launches(2);
   FEAB_CHECK_LAUNCH();
   return FEAB_OK;
 }

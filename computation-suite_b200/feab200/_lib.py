@@ -112,6 +112,7 @@ SIGNATURES = {
     "feab_gram_workspace_bytes": (_SZ, [_I64, _I32]),
     "feab_gram_bf16x3": (_I32, [_P, _I64, _I32, _P, _P, _SZ, _P, _P]),
     "feab_gram_fp64": (_I32, [_P, _I32, _I64, _I32, _P, _P, _SZ, _P]),
+    "feab_gram_int8": (_I32, [_P, _I64, _I32, _P, _P, _SZ, _P, _P]),
     "feab_symeig_jacobi": (_I32, [_P, _I32, _P, _P, _I32, _P, _P]),
     "feab_hex8_simp_vjp": (_I32, [_P, _P, _I64, C.POINTER(_D), _P, _D, _D, _P, _P, _P, _P, _P]),
     "feab_element_centroids": (_I32, [_P, _P, _I64, _P, _P]),

@@ -11,7 +11,10 @@ U = X V / sigma.  Two Gram kernels:
   elastic solutions) to FP32-input accuracy;
 * ``gram="bf16x3"``: the tensor cores (split-bf16 x3 products, FP32 accumulate, FP64 across
   chunks; feab_gram_bf16x3) -- resolves eigenvalues down to ~1e-6 of the largest, i.e. the
-  leading singular values only.
+  leading singular values only;
+* ``gram="int8"``: the tensor cores with exact products (seven signed 7-bit digits per value,
+  tcgen05.mma kind::i8 with int32 accumulation, FP64 combination; feab_gram_int8) -- FP64-level
+  accuracy at tensor-core speed.
 """
 from __future__ import annotations
 
@@ -48,6 +51,30 @@ def gram_bf16x3(X, check=True, workspace=None):
         return G, err
     if int(err.item()):
         raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
+    return G
+
+
+def gram_int8(X, check=True, workspace=None):
+    """G = X^T X (FP64, 64 x 64) of a device panel X (n x 64, FP32, row major) on the tensor cores
+    with exact integer digit products (feab_gram_int8): FP64-level accuracy.  With check=False
+    the call stays asynchronous and returns (G, error_flag) as gram_bf16x3 does."""
+    X = X.contiguous()
+    if X.dtype != torch.float32 or X.ndim != 2 or X.shape[1] != MAX_SNAPSHOTS:
+        raise ValueError("gram_int8 needs an (n, 64) float32 device panel")
+    dev = X.device
+    n = X.shape[0]
+    wbytes = int(L.lib.feab_gram_workspace_bytes(n, MAX_SNAPSHOTS))
+    ws = workspace if workspace is not None and workspace.numel() >= wbytes else torch.empty(wbytes, dtype=torch.uint8,
+                                                                                               device=dev)
+    G = torch.empty((MAX_SNAPSHOTS, MAX_SNAPSHOTS), dtype=torch.float64, device=dev)
+    err = torch.zeros(1, dtype=torch.int32, device=dev)
+    rc = L.lib.feab_gram_int8(L.dptr(X), n, MAX_SNAPSHOTS, L.dptr(G), L.dptr(ws), wbytes, L.dptr(err),
+                              L.stream_ptr(dev))
+    L.raise_for(rc, "gram_int8")
+    if not check:
+        return G, err
+    if int(err.item()):
+        raise RuntimeError("gram_int8: a bounded wait timed out on the device")
     return G
 
 
@@ -117,12 +144,12 @@ class PodBasis:
         n, k = X.shape
         if k > MAX_SNAPSHOTS:
             raise NotImplementedError(f"PodBasis.fit: at most {MAX_SNAPSHOTS} snapshots per panel on the GPU path")
-        if gram not in ("fp64", "bf16x3"):
-            raise ValueError("gram must be 'fp64' or 'bf16x3'")
-        dt = torch.float32 if gram == "bf16x3" else torch.float64
+        if gram not in ("fp64", "bf16x3", "int8"):
+            raise ValueError("gram must be 'fp64', 'bf16x3' or 'int8'")
+        dt = torch.float64 if gram == "fp64" else torch.float32
         Xp = torch.zeros((n, MAX_SNAPSHOTS), dtype=dt, device=dev)
         Xp[:, :k] = X.to(dt)
-        G = gram_bf16x3(Xp) if gram == "bf16x3" else gram_fp64(Xp)
+        G = {"bf16x3": gram_bf16x3, "int8": gram_int8, "fp64": gram_fp64}[gram](Xp)
         w, V = symeig(G)
         S = torch.sqrt(torch.clamp(w[: min(k, n)], min=0.0))
         S_host = S.cpu().numpy()

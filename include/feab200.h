@@ -344,6 +344,18 @@ size_t feab_gram_workspace_bytes(int64_t n, int32_t k);
 int32_t feab_gram_bf16x3(const float* X, int64_t n, int32_t k, double* G, void* workspace, size_t workspace_bytes,
                          int32_t* error_flag, cudaStream_t stream);
 
+/* G = X^T X (64 x 64, FP64) on the tensor cores with exact products: X (n x 64, FP32, row major,
+ * 16-byte aligned) is split per CTA row range and column into seven signed 7-bit integer digits
+ * below a power-of-two column scale, the digit products are summed exactly in int32 by
+ * tcgen05.mma kind::i8, and the scaled sums are combined in FP64 (the integer-slice method of
+ * Ootomo, Ozaki & Yokota 2024).  Inputs keep 49 bits below their CTA's column maximum, so G has
+ * FP64-level accuracy -- enough for the trailing singular values of PodBasis._fit_standard's FP64
+ * SVD (rom_engine/src/rom_engine/pod.py:140-147).  The workspace of feab_gram_bf16x3;
+ * *error_flag (device int, zero it first) is set if a bounded wait timed out.  Asynchronous;
+ * deterministic. */
+int32_t feab_gram_int8(const float* X, int64_t n, int32_t k, double* G, void* workspace, size_t workspace_bytes,
+                       int32_t* error_flag, cudaStream_t stream);
+
 /* G = X^T X (64 x 64, FP64) accumulated in FP64 on the CUDA cores, for X (n x 64, row major)
  * of FP32 (x_bytes = 4) or FP64 (x_bytes = 8) values; the same workspace as feab_gram_bf16x3.
  * The accurate Gram for snapshot sets whose spectrum decays faster than FP32 accumulation

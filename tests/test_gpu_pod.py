@@ -89,3 +89,51 @@ def test_pod_on_solution_snapshots():
     s16 = PodBasis().fit(X, n_modes=10, gram="bf16x3").singular_values
     rel16 = np.abs(s16[:10] - ref[:10]) / ref[:10]
     assert rel16[0] < 1e-5 and np.all(rel16[:5] < 1e-3), rel16
+
+
+@pytest.mark.parametrize("n", [64 * 37 + 19, 200_003])
+def test_gram_int8_is_exact_to_fp64_level(n):
+    """The integer-digit tensor-core Gram against an FP64 Gram of the same FP32 panel: columns
+    with six decades of scale, a ragged last chunk, more row ranges than CTAs."""
+    from feab200.pod import gram_int8
+    rng = np.random.default_rng(7)
+    X = (rng.standard_normal((n, 64)) * np.logspace(0, -6, 64)[None, :]).astype(np.float32)
+    G = gram_int8(torch.as_tensor(X).cuda()).cpu().numpy()
+    ref = X.astype(np.float64).T @ X.astype(np.float64)
+    scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref)))
+    assert (np.abs(G - ref) / scale).max() < 1e-13
+    assert np.array_equal(G, G.T)
+    Xt = torch.as_tensor(X).cuda()
+    assert torch.equal(gram_int8(Xt), gram_int8(Xt))       # deterministic
+
+
+def test_gram_int8_zero_and_tiny_columns():
+    from feab200.pod import gram_int8
+    rng = np.random.default_rng(8)
+    X = rng.standard_normal((5000, 64)).astype(np.float32)
+    X[:, 3] = 0.0
+    X[:, 5] *= 1e-30
+    X[100:, 7] = 0.0
+    G = gram_int8(torch.as_tensor(X).cuda()).cpu().numpy()
+    ref = X.astype(np.float64).T @ X.astype(np.float64)
+    assert np.all(G[3] == 0) and np.all(G[:, 3] == 0)
+    scale = np.sqrt(np.outer(np.diag(ref), np.diag(ref))) + 1e-300
+    ok = scale > 0
+    assert (np.abs(G - ref)[ok] / scale[ok]).max() < 1e-13
+
+
+def test_pod_int8_gram_matches_the_fp64_svd_on_a_decaying_spectrum():
+    """Snapshots with the decay of elastic solutions (sigma_10 / sigma_1 ~ 1e-4): the int8 Gram
+    keeps sigma_1..sigma_10 at FP64-Gram accuracy, where bf16x3 loses sigma_3 on."""
+    from feab200.pod import PodBasis
+    rng = np.random.default_rng(9)
+    n = 120_000
+    U, _ = np.linalg.qr(rng.standard_normal((n, 16)))
+    s = np.logspace(0, -5, 16)
+    X = ((U * s) @ np.linalg.qr(rng.standard_normal((16, 16)))[0]).astype(np.float32)
+    ref = np.linalg.svd(X.astype(np.float64), compute_uv=False)[:10]
+    got = {g: PodBasis().fit(torch.as_tensor(X).cuda(), n_modes=10, gram=g).singular_values[:10]
+           for g in ("int8", "fp64")}
+    err = {g: np.abs(v - ref) / ref for g, v in got.items()}
+    assert err["int8"].max() < 1e-7, err
+    assert err["int8"].max() <= 10 * err["fp64"].max() + 1e-12

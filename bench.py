@@ -466,6 +466,7 @@ def workload_simp(args):
     torch.autograd.Function (forward solve + adjoint solve + VJP kernel)."""
     import torch
     from feab200 import cantilever, topopt
+    from feab200._lib import KE_FULL as L_KE_FULL
     from feab200.device import DeviceMesh
     c = cantilever.simp_cantilever(96, 32, 32)
     dev = torch.device("cuda", torch.cuda.current_device())
@@ -493,23 +494,38 @@ def workload_simp(args):
     rng = np.random.default_rng(0)
     elems = rng.choice(len(rho0), 32, replace=False)
     h = 1e-6
+    # C(rho) to ~1e-18 of itself for single-element perturbations: u from the FP64 solve (relative
+    # residual 1e-13), C as the stationary form f.u + r.u with r = f - K(rho) u formed in 80-bit
+    # extended precision on the host: K(rho0) plus the perturbed element's (s(rho_e) - s(rho0_e)) ke_e.
+    # In FP64 the cancellation in K u (|K||u| ~ 1e4 |K u|) leaves ~1e-15 C of round-off, too much
+    # for differences of ~1e-11 C over h = 1e-6.
+    K0 = prob.operator(rho0).to_scipy()
+    K0_ld, K0_idx, K0_starts = K0.data.astype(np.longdouble), K0.indices, K0.indptr[:-1]
+    ke_sel = dm.element_stiffness(c.D, layout=L_KE_FULL)[torch.as_tensor(elems).to(dev)].cpu().numpy()
+    pos = np.full(3 * dm.n_nodes, -1)
+    pos[c.free] = np.arange(len(c.free))
+    f_ld = c.F[c.free].astype(np.longdouble)
+    rho0_h = rho0.cpu().numpy()
+    simp_s = lambda r: 1e-9 + (1.0 - 1e-9) * r ** 3  # noqa: E731
 
-    def compliance(rho):
-        # the stationary estimate 2 f.u - u.K u = f.u + r.u (r = f - K u): its error is quadratic in
-        # the solve error, so central differences of it resolve one element's sensitivity
-        from feab200.device import spmv
-        op = prob.operator(rho)
-        u = prob.solve_free(rho, f)
-        r = f - spmv(op, u, "fp64", lanes_per_group=8)
-        return float(torch.dot(f, u) + torch.dot(r, u))
+    def compliance(rho, q):
+        e = int(elems[q])
+        ul = prob.solve_free(rho, f).cpu().numpy().astype(np.longdouble)
+        Ku = np.add.reduceat(K0_ld * ul[K0_idx], K0_starts)
+        rows = pos[3 * c.mesh.elements[e][:, None] + np.arange(3)[None, :]].reshape(-1)
+        ue = np.where(rows >= 0, ul[np.maximum(rows, 0)], 0)
+        ds = np.longdouble(simp_s(float(rho[e])) - simp_s(rho0_h[e]))
+        kv = (ke_sel[q].astype(np.longdouble) @ ue) * ds
+        np.add.at(Ku, rows[rows >= 0], kv[rows >= 0])
+        return float(np.dot(f_ld, ul) + np.dot(f_ld - Ku, ul))
 
     def central(h):
         out = []
-        for e in elems:
+        for q, e in enumerate(elems):
             rp, rm = rho0.clone(), rho0.clone()
             rp[e] += h
             rm[e] -= h
-            out.append((compliance(rp) - compliance(rm)) / (2 * h))
+            out.append((compliance(rp, q) - compliance(rm, q)) / (2 * h))
         return np.array(out)
 
     fd, fd4 = central(h), central(1e-4)
@@ -524,8 +540,8 @@ def workload_simp(args):
                         "mixed_grad_vs_fd_h1e-4_32_elements": float(np.linalg.norm(ge - fd4) / np.linalg.norm(fd4)),
                         "mixed_grad_vs_fd_h1e-4_max_elementwise": float(np.max(np.abs(ge - fd4)[big] / np.abs(fd4)[big])),
                         "fd": ("central differences at 32 random elements, FP64 solves to 1e-13, stationary compliance "
-                               "2 f.u - u.K u; at h = 1e-6 the FP64 round-off of C(rho +- h) (about 1e-16 C against "
-                               "differences of 1e-11 C) bounds the agreement to ~1e-3; h = 1e-4 resolves it")}}
+                               "f.u + r.u with the residual r = f - K u formed in 80-bit extended precision on the "
+                               "host")}}
 
 
 def workload_batch(args):

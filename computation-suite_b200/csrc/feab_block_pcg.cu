@@ -38,15 +38,7 @@ constexpr int kModeReliable = 1;
 struct ProbState {  // per problem
   int32_t mode, pending, psel, done, status, iters, reliable, last_reliable;
   uint32_t ticket_a, ticket_b;
-  int32_t fp64vals, pad;  // mixed: the problem has switched to the FP64 values (see kFloorFraction)
 };
-
-// Mixed: at an FP64 residual replacement, |r_FP64 - r_recursive| / |b| of a column estimates the
-// residual floor of the 48-bit operator, |(K - K~) x| / |b| (the recursive residual follows the
-// 48-bit operator since the previous replacement).  A problem whose estimate exceeds this fraction
-// of the tolerance cannot reach the tolerance at FP64's iteration count on K~ (it would need an
-// extra refinement cycle), so it continues on the FP64 values from there on.
-constexpr double kFloorFraction = 0.25;
 
 // Mixed: fewest CG steps between two FP64 residual replacements of a problem, unless every
 // unconverged column is ready for one (a replacement is an FP64 SpMM over the whole panel).
@@ -333,6 +325,169 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
   }
 }
 
+// ---------------------------------------------------------------- pipelined group staging
+// 1: in the SpMM of step A (panels of 32 or 64 columns), a warp copies the next row group's
+// columns and values into shared memory with cp.async while it gathers and multiplies the current
+// one (two raw stages per warp, dynamic shared memory), so the staging latency is off the
+// critical path.  The difference form's 48-bit values are copied as stored and decoded when read.
+#ifndef FEAB_BLOCK_PIPE
+#define FEAB_BLOCK_PIPE 0
+#endif
+
+struct __align__(16) RawStage {  // the same size as GroupStage, which it stands in for
+  int col[kStageCols];
+  union {
+    double v64[3][kStageCols];
+    struct {
+      uint32_t hi[3][kStageCols];
+      uint16_t lo[3][kStageCols];
+    } d;
+  };
+};
+static_assert(sizeof(RawStage) == sizeof(GroupStage), "a raw stage doubles as a synchronous stage");
+
+__device__ __forceinline__ uint32_t shared_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
+// Start the copies of group g's columns and values into st; false (nothing issued) when the
+// group does not fit one stage.  Rows the group does not have are zero-filled.
+template <bool DIFF>
+__device__ __forceinline__ bool stage_issue(const BArgs& A, int g, int lane, RawStage& st) {
+  const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+  if (DIFF) {
+    const int c0 = A.goff[g], s0 = A.voff[g], len = A.goff[g + 1] - c0;
+    if (len > kStageCols) return false;
+    for (int mq = lane; mq < (len >> 2); mq += 32) {
+      const int m = 4 * mq;
+      cp_async16(&st.col[m], A.tcol + c0 + m);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k < f) {
+          cp_async16(&st.d.hi[k][m], A.vhi + s0 + k * len + m);
+          cp_async8(&st.d.lo[k][m], A.vlo + s0 + k * len + m);
+        } else {
+          *reinterpret_cast<uint4*>(&st.d.hi[k][m]) = make_uint4(0u, 0u, 0u, 0u);
+          *reinterpret_cast<uint2*>(&st.d.lo[k][m]) = make_uint2(0u, 0u);
+        }
+      }
+    }
+  } else {
+    const int s0 = A.row_ptr[r0], len = A.row_ptr[r0 + 1] - s0;
+    if (len > kStageCols) return false;
+    for (int m = lane; m < len; m += 32) {
+      cp_async4(&st.col[m], A.col_idx + s0 + m);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (k < f) cp_async8(&st.v64[k][m], A.vals64 + s0 + k * len + m);
+        else st.v64[k][m] = 0.0;
+      }
+    }
+  }
+  cp_async_commit();
+  return true;
+}
+
+// The SpMM of group g from a stage filled by stage_issue (one sub-warp, K >= 32).
+template <int K, bool DIFF>
+__device__ __forceinline__ void group_spmm_staged(const BArgs& A, int g, int lane, const RawStage& st,
+                                                  const double* __restrict__ src, double (&acc)[3][K / 32]) {
+  constexpr int CPL = K / 32;
+  const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+  const int nc = DIFF ? A.goff[g + 1] - A.goff[g] : A.row_ptr[r0 + 1] - A.row_ptr[r0];
+#pragma unroll
+  for (int k = 0; k < 3; ++k)
+#pragma unroll
+    for (int q = 0; q < CPL; ++q) acc[k][q] = 0.0;
+  double xs[3][CPL];
+  if (DIFF) {
+    const int mask = A.gmask[g];
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+      if ((mask >> j) & 1) {
+        gather_row<K>(src, r0 + __popc(mask & ((1 << j) - 1)), lane, xs[j]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) xs[j][q] = 0.0;
+      }
+    }
+  }
+  for (int m0 = 0; m0 < nc; m0 += kUnroll) {
+    unsigned t[kUnroll];
+    double xv[kUnroll][CPL];
+#pragma unroll
+    for (int u4 = 0; u4 < kUnroll / 4; ++u4) {
+      const int4 tq = *reinterpret_cast<const int4*>(&st.col[m0 + 4 * u4]);
+      t[4 * u4] = (unsigned)tq.x;
+      t[4 * u4 + 1] = (unsigned)tq.y;
+      t[4 * u4 + 2] = (unsigned)tq.z;
+      t[4 * u4 + 3] = (unsigned)tq.w;
+    }
+#pragma unroll
+    for (int u = 0; u < kUnroll; ++u) {
+      if (m0 + u < nc) {
+        gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), lane, xv[u]);
+      } else {
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;
+      }
+    }
+#pragma unroll
+    for (int u2 = 0; u2 < kUnroll / 2; ++u2) {
+      const int m = m0 + 2 * u2;
+      if (m >= nc) break;
+      double2 w[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        if (DIFF) {
+          const uint2 h = *reinterpret_cast<const uint2*>(&st.d.hi[k][m]);
+          const uint32_t l = *reinterpret_cast<const uint32_t*>(&st.d.lo[k][m]);
+          w[k] = make_double2(dec48(h.x, (uint16_t)(l & 0xffffu)), dec48(h.y, (uint16_t)(l >> 16)));
+        } else {
+          w[k] = *reinterpret_cast<const double2*>(&st.v64[k][m]);
+        }
+      }
+      const bool two = m + 1 < nc;  // a column past nc has xv = 0 but a stale value
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const double d = xv[2 * u2][q];
+        acc[0][q] = fma(w[0].x, d, acc[0][q]);
+        acc[1][q] = fma(w[1].x, d, acc[1][q]);
+        acc[2][q] = fma(w[2].x, d, acc[2][q]);
+      }
+      if (two) {
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) {
+          const double d = xv[2 * u2 + 1][q];
+          acc[0][q] = fma(w[0].y, d, acc[0][q]);
+          acc[1][q] = fma(w[1].y, d, acc[1][q]);
+          acc[2][q] = fma(w[2].y, d, acc[2][q]);
+        }
+      }
+    }
+  }
+  if (DIFF) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      if (k < f) {
+        const double s0v = A.S[(int64_t)(r0 + k) * 3 + 0], s1v = A.S[(int64_t)(r0 + k) * 3 + 1],
+                     s2v = A.S[(int64_t)(r0 + k) * 3 + 2];
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) acc[k][q] += s0v * xs[0][q] + s1v * xs[1][q] + s2v * xs[2][q];
+      }
+    }
+  }
+}
+
 // setup: R = B - 0 (x0 = 0), P = M R, per column ||b||, r.z; columns beyond the problem's
 // RHS count are inactive from the start.
 template <int K>
@@ -393,7 +548,6 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
         P.iters = 0;
         P.reliable = 0;
         P.last_reliable = 0;
-        P.fp64vals = 0;
         P.status = FEAB_OK;
         P.done = all;
         if (all) atomicSub(A.remaining, 1);
@@ -409,24 +563,53 @@ template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
+  constexpr bool PIPE = FEAB_BLOCK_PIPE && K >= 32;
   __shared__ double sm[kWarps][K];
-  __shared__ double smg[MIXED ? kWarps : 1][K];
-  __shared__ GroupStage stage[kWarps];
-  __shared__ int switch_vals;
+  __shared__ GroupStage stage[PIPE ? 1 : kWarps];
+  extern __shared__ __align__(16) unsigned char dyn_stage[];  // PIPE: two raw stages per warp
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  RawStage* rs = reinterpret_cast<RawStage*>(dyn_stage) + 2 * w;
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
     const ProbState P = A.ps[p];
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
+    const bool diff = MIXED && !reliable;
     const double* __restrict__ po = A.P0;  // the direction, already updated by k_bstep_p
-    double part[CPL], gap[CPL];
+    const double* __restrict__ src = reliable ? A.X : po;
+    double part[CPL];
 #pragma unroll
-    for (int q = 0; q < CPL; ++q) part[q] = gap[q] = 0.0;
-    for (int g = A.item_g0[it] + w; g < A.item_g1[it]; g += kWarps) {
+    for (int q = 0; q < CPL; ++q) part[q] = 0.0;
+    const int g1 = A.item_g1[it];
+    int buf = 0;
+    bool staged = false;
+    if constexpr (PIPE) {
+      const int g = A.item_g0[it] + w;
+      if (g < g1) staged = diff ? stage_issue<true>(A, g, lane, rs[0]) : stage_issue<false>(A, g, lane, rs[0]);
+    }
+    for (int g = A.item_g0[it] + w; g < g1; g += kWarps) {
       double acc[3][CPL];
-      if constexpr (MIXED) {
-        if (reliable || P.fp64vals) group_spmm<K, false>(A, g, lane, stage[w], reliable ? A.X : po, acc);
+      if constexpr (PIPE) {
+        // group g's copies have landed; start group g + kWarps's into the other stage
+        cp_async_wait_all();
+        __syncwarp();
+        bool staged_next = false;
+        const int gn = g + kWarps;
+        if (gn < g1)
+          staged_next = diff ? stage_issue<true>(A, gn, lane, rs[buf ^ 1]) : stage_issue<false>(A, gn, lane, rs[buf ^ 1]);
+        if (staged) {
+          if (diff) group_spmm_staged<K, true>(A, g, lane, rs[buf], src, acc);
+          else group_spmm_staged<K, false>(A, g, lane, rs[buf], src, acc);
+        } else {
+          GroupStage& gs = *reinterpret_cast<GroupStage*>(&rs[buf]);
+          if (diff) group_spmm<K, MIXED>(A, g, lane, gs, src, acc);
+          else group_spmm<K, false>(A, g, lane, gs, src, acc);
+        }
+        __syncwarp();  // every lane is done with rs[buf] before it is refilled
+        staged = staged_next;
+        buf ^= 1;
+      } else if constexpr (MIXED) {
+        if (!diff) group_spmm<K, false>(A, g, lane, stage[w], src, acc);
         else group_spmm<K, true>(A, g, lane, stage[w], po, acc);
       } else {
         group_spmm<K, false>(A, g, lane, stage[w], po, acc);
@@ -441,10 +624,8 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
             const int64_t idx = (int64_t)(r0 + k) * K + panel_col<K>(lane, q);
             if (reliable) {
               const double ri = A.B[idx] - acc[k][q];
-              const double d = ri - A.R[idx];  // FP64 minus recursive residual
               A.R[idx] = ri;
               part[q] += ri * ri;
-              gap[q] += d * d;
             } else {
               const double pv = po[idx];
               A.AP[idx] = acc[k][q];
@@ -456,36 +637,23 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
     }
     if (lane < LW) {
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) {
-        sm[w][panel_col<K>(lane, q)] = part[q];
-        if constexpr (MIXED) smg[w][panel_col<K>(lane, q)] = gap[q];
-      }
+      for (int q = 0; q < CPL; ++q) sm[w][panel_col<K>(lane, q)] = part[q];
     }
     __syncthreads();
     if (threadIdx.x < K) {
-      double s = 0.0, sg = 0.0;
-      for (int q = 0; q < kWarps; ++q) {
-        s += sm[q][threadIdx.x];
-        if constexpr (MIXED) sg += smg[q][threadIdx.x];
-      }
+      double s = 0.0;
+      for (int q = 0; q < kWarps; ++q) s += sm[q][threadIdx.x];
       A.part[(int64_t)it * 2 * K + threadIdx.x] = s;
-      if (reliable) A.part[(int64_t)it * 2 * K + K + threadIdx.x] = sg;
     }
     const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
     if (last_of_problem(&A.ps[p].ticket_a, n_it)) {
-      if (threadIdx.x == 0) switch_vals = 0;
-      __syncthreads();
       if (threadIdx.x < K) {
         const int c = threadIdx.x;
-        double s = 0.0, sg = 0.0;
-        for (int q = 0; q < n_it; ++q) {
-          s += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
-          if (reliable) sg += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + K + c]);
-        }
+        double s = 0.0;
+        for (int q = 0; q < n_it; ++q) s += __ldcg(&A.part[(int64_t)(i0 + q) * 2 * K + c]);
         ColState& C = A.cs[(int64_t)p * K + c];
         if (reliable) {
           C.rr = s;
-          if (C.active && !C.converged && sqrt(sg) > kFloorFraction * A.tol * C.bnorm) atomicOr(&switch_vals, 1);
         } else {
           C.alpha = 0.0;
           if (C.active && !C.converged) {
@@ -498,7 +666,6 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
       if (threadIdx.x == 0) {
         ProbState& Pm = A.ps[p];
         Pm.ticket_a = 0;
-        if (switch_vals) Pm.fp64vals = 1;
         if (!reliable) {
           Pm.pending = 0;
           if (Pm.status != FEAB_OK) {
@@ -847,15 +1014,20 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   };
   do {
     if (fail(graphs.events(ev))) break;
+    const size_t smem_a = (FEAB_BLOCK_PIPE && K >= 32) ? 2 * kWarps * sizeof(RawStage) : 0;
+    if (smem_a) {
+      if (fail(cudaFuncSetAttribute(k_bstep_a<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
+      if (fail(cudaFuncSetAttribute(k_bstep_a<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
+    }
     auto record = [&](cudaStream_t cs) {
       for (int q = 0; q < chunk; ++q) {
         if (prec == FEAB_PREC_MIXED) {
           k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
-          k_bstep_a<K, true><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_a<K, true><<<grid, kThreads, smem_a, cs>>>(A);
           k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
         } else {
           k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
-          k_bstep_a<K, false><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_a<K, false><<<grid, kThreads, smem_a, cs>>>(A);
           k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
         }
       }

@@ -589,7 +589,7 @@ def workload_snapshot(args):
     import torch
     from feab200 import cantilever
     from feab200.batched import ProblemBatch
-    from feab200.pod import gram_bf16x3, gram_fp64, symeig
+    from feab200.pod import gram_bf16x3, gram_fp64, gram_int8, symeig
     c = cantilever.fourier_snapshot_cantilever(*args.snapshot_shape)
     b = ProblemBatch([(c.mesh.nodes, c.mesh.elements, c.D, c.fixed, c.F)])
     t0 = time.perf_counter()
@@ -615,6 +615,11 @@ def workload_snapshot(args):
     if int(gflag.item()):
         raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
     gram64_ms, G64 = _timed(lambda: gram_fp64(X32), 5, 2)
+    gram8_ms, (G8, g8flag) = _timed(lambda: gram_int8(X32, check=False), 5, 2)
+    if int(g8flag.item()):
+        raise RuntimeError("gram_int8: a bounded wait timed out on the device")
+    w8, _ = symeig(G8)
+    s_gpu8 = torch.sqrt(torch.clamp(w8, min=0)).cpu().numpy()
     eig_ms, (w, V) = _timed(lambda: symeig(G), 3, 1)
     w64, _ = symeig(G64)
     s_gpu = torch.sqrt(torch.clamp(w, min=0)).cpu().numpy()
@@ -623,6 +628,8 @@ def workload_snapshot(args):
     s_ref = O.pod_singular_values(X.cpu().numpy())
     rel = np.abs(s_gpu[:10] - s_ref[:10]) / s_ref[:10]
     rel64 = np.abs(s_gpu64[:10] - s_ref[:10]) / s_ref[:10]
+    rel8 = np.abs(s_gpu8[:10] - s_ref[:10]) / s_ref[:10]
+    rel8_vs_64 = np.abs(s_gpu8[:10] - s_gpu64[:10]) / s_gpu64[:10]
     n, k = X.shape
     peak, _ = measured_peak()
     gram_bytes = n * k * 4 + k * k * 8
@@ -639,6 +646,14 @@ def workload_snapshot(args):
             "n_free": n, "rhs": int(c.F.shape[1]), "iters_max": int(res["mixed"][2].iters.max()),
             "sigma_rel_err_top10_bf16x3": [float(v) for v in rel],
             "sigma_rel_err_top10_fp64_gram": [float(v) for v in rel64],
+            "sigma_rel_err_top10_int8_gram": [float(v) for v in rel8],
+            "sigma_int8_vs_fp64_gram_top10": [float(v) for v in rel8_vs_64],
+            "gram_int8_ms": round(gram8_ms, 4),
+            "gram_int8_roofline": {"bound": "hbm", "achieved": round(2 * n * k * 4 / (gram8_ms * 1e-3) / 1e9, 1),
+                                   "peak": peak, "unit": "GB/s",
+                                   "frac": round(2 * n * k * 4 / (gram8_ms * 1e-3) / 1e9 / peak, 3),
+                                   "bytes_per_launch": int(2 * n * k * 4),
+                                   "note": "X read twice (column scales, then the digits)"},
             "sigma_over_sigma1_top10": [float(v) for v in s_ref[:10] / s_ref[0]],
             "gram_fp64_ms": round(gram64_ms, 4),
             "pod_value_uses": "FP64 Gram (PodBasis default); bf16x3 tensor-core Gram timed and checked beside it",
@@ -646,50 +661,56 @@ def workload_snapshot(args):
 
 
 def workload_gram(args):
-    """The tensor-core Gram (and, beside it, the FP64 CUDA-core Gram) alone on a seeded random
-    1,382,976 x 64 FP32 panel (the snapshot set's size), L2 flushed before each timed launch."""
+    """The tensor-core Grams alone on a seeded random 1,382,976 x 64 FP32 panel (the snapshot set's
+    size), L2 flushed before each timed launch: the exact-product int8 Gram (the headline of this
+    line), the split-bf16 Gram and the FP64 CUDA-core Gram beside them, each against an FP64
+    Gram of the same panel."""
     import torch
-    from feab200.pod import gram_bf16x3, gram_fp64, symeig
+    from feab200.pod import gram_bf16x3, gram_fp64, gram_int8
     n, k = 1_382_976, 64
     g = torch.Generator(device="cuda").manual_seed(5)
     X = torch.randn((n, k), generator=g, device="cuda", dtype=torch.float32)
     flush = L2Flush("cuda")
     ws = torch.empty(int(__import__("feab200")._lib.lib.feab_gram_workspace_bytes(n, k)), dtype=torch.uint8,
                      device="cuda")
+    kernels = {"int8": lambda: gram_int8(X, check=False, workspace=ws),
+               "bf16x3": lambda: gram_bf16x3(X, check=False, workspace=ws),
+               "fp64": lambda: (gram_fp64(X, workspace=ws), None)}
     for _ in range(args.warmup):
-        gram_bf16x3(X)
-    times, times64, flags = [], [], []
+        for fn in kernels.values():
+            fn()
+    times = {name: [] for name in kernels}
+    out = {}
     for _ in range(args.steps):
-        for fn, out in ((lambda: gram_bf16x3(X, check=False, workspace=ws), times),
-                        (lambda: gram_fp64(X, workspace=ws), times64)):
+        for name, fn in kernels.items():
             flush()
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
-            r = fn()
+            G, f = fn()
             b.record()
             torch.cuda.synchronize()
-            out.append(a.elapsed_time(b))
-            if isinstance(r, tuple):
-                G, f = r
-                flags.append(int(f.item()))
-    if any(flags):
-        raise RuntimeError("gram_bf16x3: a bounded wait timed out on the device")
-    ms64 = statistics.mean(times64)
-    G64 = gram_fp64(X)
-    ms = statistics.mean(times)
+            times[name].append(a.elapsed_time(b))
+            if f is not None and int(f.item()):
+                raise RuntimeError(f"gram_{name}: a bounded wait timed out on the device")
+            out[name] = G
     ref = X.double().T @ X.double()
-    err = float((G - ref).abs().max() / ref.abs().max())
-    w, _ = symeig(G)
+    scale = torch.sqrt(torch.outer(torch.diagonal(ref), torch.diagonal(ref)))
     peak, kind = measured_peak()
-    nbytes = n * k * 4 + k * k * 8
-    return {"metric": "tensor-core split-bf16 Gram X^T X time, 1382976 x 64 FP32", "value": round(ms, 4), "unit": "ms",
+    res = {}
+    for name in kernels:
+        ms = statistics.mean(times[name])
+        nbytes = n * k * 4 * (2 if name == "int8" else 1) + k * k * 8
+        res[name] = {"ms": round(ms, 4), "max_rel_err_vs_fp64_product": float(((out[name] - ref).abs() / scale).max()),
+                     "achieved_gbs": round(nbytes / (ms * 1e-3) / 1e9, 1), "bytes_per_launch": nbytes}
+    ms = res["int8"]["ms"]
+    nbytes = res["int8"]["bytes_per_launch"]
+    return {"metric": "tensor-core exact-product (int8 digits) Gram X^T X time, 1382976 x 64 FP32", "value": ms,
+            "unit": "ms",
             "roofline": {"bound": "hbm", "achieved": round(nbytes / (ms * 1e-3) / 1e9, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(nbytes / (ms * 1e-3) / 1e9 / peak, 3), "bytes_per_launch": nbytes,
-                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})"},
-            "gram_rel_err_vs_fp64": err, "lambda_max": float(w[0]),
-            "gram_fp64_cuda_cores_ms": round(ms64, 4),
-            "gram_fp64_rel_err_vs_fp64": float((G64 - ref).abs().max() / ref.abs().max()),
-            "timing": "CUDA events around the kernel launches only, L2 flushed before each"}
+                         "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})",
+                         "note": "X is read twice (column scales, then the digits)"},
+            "kernels": res, "timing": "CUDA events around each launch, L2 flushed before each"}
 
 
 def workload_spmv(args):

@@ -79,14 +79,24 @@ struct BArgs {
   int32_t maxiter;
 };
 
-__device__ __forceinline__ bool last_of_problem(uint32_t* ticket, int n_items_p) {
+// True in the block that completes the last of problem p's n_items_p work items; `count` items
+// are completed by this call.
+__device__ __forceinline__ bool last_of_problem(uint32_t* ticket, int n_items_p, int count = 1) {
   __shared__ bool last;
   __threadfence();
   __syncthreads();
-  if (threadIdx.x == 0) last = (atomicAdd(ticket, 1u) == (uint32_t)(n_items_p - 1));
+  if (threadIdx.x == 0) last = (atomicAdd(ticket, (uint32_t)count) == (uint32_t)(n_items_p - count));
   __syncthreads();
   return last;
 }
+
+// The vector passes P and B take runs of up to kBRun consecutive work items of one problem as
+// one contiguous row range (the items of a problem cover consecutive row groups), which cuts
+// their per-item block reductions and tickets; the SpMM keeps the finer items for its balance.
+#ifndef FEAB_BLOCK_BRUN
+#define FEAB_BLOCK_BRUN 1
+#endif
+constexpr int kBRun = FEAB_BLOCK_BRUN;
 
 // Block-wide per-column sums: thread t contributes v to column t % K (blockDim multiple of K).
 template <int K>
@@ -685,11 +695,15 @@ template <int K>
 __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
   double* __restrict__ P0 = A.P0;
   const double* __restrict__ R = A.R;
-  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+  for (int ru = blockIdx.x; ru * kBRun < A.n_items; ru += gridDim.x) {
+   const int it_end = min(A.n_items, (ru + 1) * kBRun);
+   for (int it = ru * kBRun, it2 = it; it < it_end; it = it2) {
     const int p = A.item_problem[it];
+    for (it2 = it + 1; it2 < it_end && A.item_problem[it2] == p; ++it2) {
+    }
     const ProbState P = A.ps[p];
     if (P.done || !P.pending) continue;
-    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
+    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it2 - 1]];
     if constexpr (K >= 2) {
       // two adjacent columns per thread with 16-byte accesses, four pairs per trip
       const int c2 = 2 * (threadIdx.x % (K / 2));
@@ -733,6 +747,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
         }
       }
     }
+   }
   }
 }
 
@@ -747,8 +762,12 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
   __shared__ double smv[2][2 * kThreads];
   __shared__ int flag_any, flag_all;
   const int c = threadIdx.x % K;
-  for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
+  for (int ru = blockIdx.x; ru * kBRun < A.n_items; ru += gridDim.x) {
+   const int it_end = min(A.n_items, (ru + 1) * kBRun);
+   for (int it = ru * kBRun, it2 = it; it < it_end; it = it2) {
     const int p = A.item_problem[it];
+    for (it2 = it + 1; it2 < it_end && A.item_problem[it2] == p; ++it2) {
+    }
     const ProbState P = A.ps[p];
     if (P.done) continue;
     const bool reliable = MIXED && P.mode == kModeReliable;
@@ -756,7 +775,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
     double* __restrict__ X = A.X;
     double* __restrict__ R = A.R;
     const double* __restrict__ AP = A.AP;
-    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it]];
+    const int r0 = A.group_ptr[A.item_g0[it]], r1 = A.group_ptr[A.item_g1[it2 - 1]];
     if constexpr (K >= 2 && FEAB_BLOCK_VECB) {
       // two adjacent columns c2, c2 + 1 per thread with 16-byte accesses, kVecU pairs per trip,
       // every load of the trip issued before any store
@@ -817,6 +836,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
       if (threadIdx.x < K) {
         A.part[(int64_t)it * 2 * K + c] = smv[0][c];
         A.part[(int64_t)it * 2 * K + K + c] = smv[1][c];
+        for (int z = it + 1; z < it2; ++z) A.part[(int64_t)z * 2 * K + c] = A.part[(int64_t)z * 2 * K + K + c] = 0.0;
       }
     } else {
       const double alpha = A.cs[(int64_t)p * K + c].alpha;
@@ -858,10 +878,11 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
       if (threadIdx.x < K) {
         A.part[(int64_t)it * 2 * K + c] = sm[0][c];
         A.part[(int64_t)it * 2 * K + K + c] = sm[1][c];
+        for (int z = it + 1; z < it2; ++z) A.part[(int64_t)z * 2 * K + c] = A.part[(int64_t)z * 2 * K + K + c] = 0.0;
       }
     }
     const int i0 = A.prob_items[p], n_it = A.prob_items[p + 1] - i0;
-    if (last_of_problem(&A.ps[p].ticket_b, n_it)) {
+    if (last_of_problem(&A.ps[p].ticket_b, n_it, it2 - it)) {
       // mixed: a column is ready for an FP64 residual replacement once its recursive residual
       // dropped by delta since the last one or reached tol; the problem replaces when a column
       // is ready and kMinReliableGap steps have passed, or when every unconverged column is ready
@@ -931,6 +952,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
       }
     }
     __syncthreads();
+   }
   }
 }
 
@@ -995,6 +1017,7 @@ template <int K>
 int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int32_t* host_iters, double* host_relres,
                   int32_t* host_status) {
   const int grid = std::max(1, std::min(A.n_items, sm_count() * 4));
+  const int grid_pb = std::max(1, std::min((A.n_items + kBRun - 1) / kBRun, sm_count() * 4));  // P and B runs
   cudaMemsetAsync(A.ps, 0, sizeof(ProbState) * A.n_problems, s);
   int32_t np = A.n_problems;
   cudaMemcpyAsync(A.remaining, &np, sizeof(int32_t), cudaMemcpyHostToDevice, s);
@@ -1022,18 +1045,18 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
     auto record = [&](cudaStream_t cs) {
       for (int q = 0; q < chunk; ++q) {
         if (prec == FEAB_PREC_MIXED) {
-          k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_p<K><<<grid_pb, kThreads, 0, cs>>>(A);
           k_bstep_a<K, true><<<grid, kThreads, smem_a, cs>>>(A);
-          k_bstep_b<K, true><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_b<K, true><<<grid_pb, kThreads, 0, cs>>>(A);
         } else {
-          k_bstep_p<K><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_p<K><<<grid_pb, kThreads, 0, cs>>>(A);
           k_bstep_a<K, false><<<grid, kThreads, smem_a, cs>>>(A);
-          k_bstep_b<K, false><<<grid, kThreads, 0, cs>>>(A);
+          k_bstep_b<K, false><<<grid_pb, kThreads, 0, cs>>>(A);
         }
       }
       cudaMemcpyAsync((void*)hflag, A.remaining, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
     };
-    if (fail(graphs.acquire(&A, sizeof(A), topo_signature({K, prec, chunk, grid}), record, &exec))) break;
+    if (fail(graphs.acquire(&A, sizeof(A), topo_signature({K, prec, chunk, grid, grid_pb}), record, &exec))) break;
     // iterations and reliable steps per problem are bounded by maxiter each
     const int64_t max_launch = (2 * (int64_t)maxiter + 2 + chunk - 1) / chunk + 1;
     hflag[0] = np;

@@ -163,7 +163,7 @@ def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=
 
 
 # ----------------------------------------------------------------------------- launch-shape tuner
-ITEM_GROUPS = (16, 32, 64, 128)
+ITEM_GROUPS = (16, 32, 64, 128, 256)
 
 
 @dataclass

@@ -18,8 +18,8 @@
 // deterministic.  Converged problems are skipped; the host polls a "problems remaining"
 // counter one CUDA-graph chunk behind.
 //
-// Precisions: FEAB_PREC_FP64 (reference recurrence) and FEAB_PREC_MIXED (SpMM on 48-bit values
-// in difference form with FP64 vectors; per problem, an FP64 residual replacement with the
+// Precisions: FEAB_PREC_FP64 (reference recurrence) and FEAB_PREC_MIXED (SpMM on 7-byte values,
+// 44-bit mantissas, in difference form with FP64 vectors; per problem, an FP64 residual replacement with the
 // FP64 values whenever a column's residual dropped by reliable_delta; convergence on the FP64
 // residual).
 #include <algorithm>
@@ -57,6 +57,7 @@ struct BArgs {
   const double* vals64;
   const uint32_t* vhi;
   const uint16_t* vlo;
+  const uint8_t* vlo2;
   const int32_t* tcol;
   const uint8_t* gmask;
   const double* S;
@@ -109,11 +110,13 @@ __device__ __forceinline__ void block_col_sums(double v, double* sm) {
   }
 }
 
-__device__ __forceinline__ double dec48(uint32_t hi, uint16_t lo) {
-  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)lo << 16)));
+// A difference-form value from its three stored parts (44 mantissa bits).
+__device__ __forceinline__ double dec56(uint32_t hi, uint32_t lo, uint32_t lo2) {
+  return __longlong_as_double((long long)(((unsigned long long)hi << 32) | ((unsigned long long)(lo & 0xffffu) << 16) |
+                                          ((unsigned long long)(lo2 & 0xffu) << 8)));
 }
 
-// A warp's staging area for one row group's columns and values (FP64, decoded from the 48-bit
+// A warp's staging area for one row group's columns and values (FP64, decoded from the 56-bit
 // form for the difference operator), filled with coalesced loads before the SpMM reads them as
 // broadcasts; groups longer than kStageCols are staged in pieces.
 constexpr int kStageCols = 128;
@@ -222,10 +225,11 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
           if (k < f) {
             const uint4 h = __ldg(reinterpret_cast<const uint4*>(A.vhi + s0 + k * len + cb + m));
             const uint2 l = __ldg(reinterpret_cast<const uint2*>(A.vlo + s0 + k * len + cb + m));
-            st.val[k][m] = dec48(h.x, (uint16_t)(l.x & 0xffffu));
-            st.val[k][m + 1] = dec48(h.y, (uint16_t)(l.x >> 16));
-            st.val[k][m + 2] = dec48(h.z, (uint16_t)(l.y & 0xffffu));
-            st.val[k][m + 3] = dec48(h.w, (uint16_t)(l.y >> 16));
+            const uint32_t l2 = __ldg(reinterpret_cast<const uint32_t*>(A.vlo2 + s0 + k * len + cb + m));
+            st.val[k][m] = dec56(h.x, l.x, l2);
+            st.val[k][m + 1] = dec56(h.y, l.x >> 16, l2 >> 8);
+            st.val[k][m + 2] = dec56(h.z, l.y, l2 >> 16);
+            st.val[k][m + 3] = dec56(h.w, l.y >> 16, l2 >> 24);
           } else {
             st.val[k][m] = st.val[k][m + 1] = st.val[k][m + 2] = st.val[k][m + 3] = 0.0;
           }
@@ -339,7 +343,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
 // 1: in the SpMM of step A (panels of 32 or 64 columns), a warp copies the next row group's
 // columns and values into shared memory with cp.async while it gathers and multiplies the current
 // one (two raw stages per warp, dynamic shared memory), so the staging latency is off the
-// critical path.  The difference form's 48-bit values are copied as stored and decoded when read.
+// critical path.  The difference form's 56-bit values are copied as stored and decoded when read.
 #ifndef FEAB_BLOCK_PIPE
 #define FEAB_BLOCK_PIPE 0
 #endif
@@ -351,6 +355,7 @@ struct __align__(16) RawStage {  // the same size as GroupStage, which it stands
     struct {
       uint32_t hi[3][kStageCols];
       uint16_t lo[3][kStageCols];
+      uint8_t lo2[3][kStageCols];
     } d;
   };
 };
@@ -385,9 +390,11 @@ __device__ __forceinline__ bool stage_issue(const BArgs& A, int g, int lane, Raw
         if (k < f) {
           cp_async16(&st.d.hi[k][m], A.vhi + s0 + k * len + m);
           cp_async8(&st.d.lo[k][m], A.vlo + s0 + k * len + m);
+          cp_async4(&st.d.lo2[k][m], A.vlo2 + s0 + k * len + m);
         } else {
           *reinterpret_cast<uint4*>(&st.d.hi[k][m]) = make_uint4(0u, 0u, 0u, 0u);
           *reinterpret_cast<uint2*>(&st.d.lo[k][m]) = make_uint2(0u, 0u);
+          *reinterpret_cast<uint32_t*>(&st.d.lo2[k][m]) = 0u;
         }
       }
     }
@@ -461,7 +468,8 @@ __device__ __forceinline__ void group_spmm_staged(const BArgs& A, int g, int lan
         if (DIFF) {
           const uint2 h = *reinterpret_cast<const uint2*>(&st.d.hi[k][m]);
           const uint32_t l = *reinterpret_cast<const uint32_t*>(&st.d.lo[k][m]);
-          w[k] = make_double2(dec48(h.x, (uint16_t)(l & 0xffffu)), dec48(h.y, (uint16_t)(l >> 16)));
+          const uint32_t l2 = *reinterpret_cast<const uint16_t*>(&st.d.lo2[k][m]);
+          w[k] = make_double2(dec56(h.x, l, l2), dec56(h.y, l >> 16, l2 >> 8));
         } else {
           w[k] = *reinterpret_cast<const double2*>(&st.v64[k][m]);
         }
@@ -1132,9 +1140,10 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   // the R / P / AP panels are carved from the workspace at 256-byte offsets and are read and
   // written with 16-byte accesses by the vector passes
   if ((reinterpret_cast<uintptr_t>(workspace) & 15) != 0) return FEAB_BAD_ARG;
-  if (D && (!D->tcol || !D->vhi || !D->vlo || (reinterpret_cast<uintptr_t>(D->tcol) & 15) ||
-            (reinterpret_cast<uintptr_t>(D->vhi) & 15) || (reinterpret_cast<uintptr_t>(D->vlo) & 7)))
-    return FEAB_BAD_ARG;  // 16-byte column / hi-word quads, 8-byte lo words
+  if (D && (!D->tcol || !D->vhi || !D->vlo || !D->vlo2 || (reinterpret_cast<uintptr_t>(D->tcol) & 15) ||
+            (reinterpret_cast<uintptr_t>(D->vhi) & 15) || (reinterpret_cast<uintptr_t>(D->vlo) & 7) ||
+            (reinterpret_cast<uintptr_t>(D->vlo2) & 3)))
+    return FEAB_BAD_ARG;  // 16-byte column / hi-word quads, 8-byte lo and 4-byte lo2 words
   const BLayout L = blayout(M->n, k, bt->n_problems, bt->n_items);
   if (L.total > workspace_bytes) return FEAB_BAD_ARG;
   char* w = static_cast<char*>(workspace);
@@ -1151,6 +1160,7 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   if (D) {
     A.vhi = D->vhi;
     A.vlo = D->vlo;
+    A.vlo2 = D->vlo2;
     A.tcol = D->tcol;
     A.gmask = D->gmask;
     A.goff = D->goff;

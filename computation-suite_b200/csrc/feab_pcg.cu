@@ -676,7 +676,8 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
                                                          const int32_t* __restrict__ goff,
                                                          const int32_t* __restrict__ voff,
                                                          int32_t* __restrict__ tcol, uint32_t* __restrict__ vhi,
-                                                         uint16_t* __restrict__ vlo, uint8_t* __restrict__ gmask,
+                                                         uint16_t* __restrict__ vlo, uint8_t* __restrict__ vlo2,
+                                                         uint8_t* __restrict__ gmask,
                                                          double* __restrict__ Ssum, int32_t* __restrict__ err) {
   const int lane = threadIdx.x & 31;
   const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -715,16 +716,17 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
         if (c < own || c >= own + f) {
           const int p = c < own ? c : c - f;
           if (k == 0) tcol[c0 + p] = (int32_t)((uint32_t)col | ((uint32_t)j << 30));
-          const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
+          const unsigned long long bits = (unsigned long long)__double_as_longlong(v) + 0x80ull;  // 44 bits
           vhi[v0 + k * lp + p] = (uint32_t)(bits >> 32);
           vlo[v0 + k * lp + p] = (uint16_t)((bits >> 16) & 0xffffull);
+          vlo2[v0 + k * lp + p] = (uint8_t)((bits >> 8) & 0xffull);
         }
       }
       // rounded value of an off-node column (0 for own columns and past the end)
       double wv = 0.0;
       if (c < len && (c < own || c >= own + f)) {
-        const unsigned long long bw = (unsigned long long)__double_as_longlong(v) + 0x8000ull;
-        wv = __longlong_as_double((long long)(bw & ~0xffffull));
+        const unsigned long long bw = (unsigned long long)__double_as_longlong(v) + 0x80ull;
+        wv = __longlong_as_double((long long)(bw & ~0xffull));
       }
       for (int u = 0; u < 32; ++u) {
         const double vu = __shfl_sync(FEAB_FULL_MASK, v, u);
@@ -741,6 +743,7 @@ __global__ void __launch_bounds__(kThreads) k_build_diff(int32_t n_groups, const
       if (k == 0) tcol[c0 + p] = (int32_t)((uint32_t)r0 | ((uint32_t)j0 << 30));
       vhi[v0 + k * lp + p] = 0u;
       vlo[v0 + k * lp + p] = 0;
+      vlo2[v0 + k * lp + p] = 0;
     }
     // T = S - W (S: all exact values of component j, W: the rounded off-node ones), so that
     // sum_{b != a} w (x_b - x_a) + S x_a = sum_{b != a} w x_b + T x_a exactly
@@ -1010,6 +1013,7 @@ void diff_layout(int32_t n, int64_t nnz, int32_t n_groups, char* base, feab_diff
   char* tc = take(sizeof(int32_t) * ncol);
   char* hi = take(sizeof(uint32_t) * nval);
   char* lo = take(sizeof(uint16_t) * nval);
+  char* lo2 = take(sizeof(uint8_t) * nval);
   char* gm = take((size_t)n_groups);
   char* ss = take(sizeof(double) * 3 * (size_t)n);
   char* go = take(sizeof(int32_t) * ((size_t)n_groups + 1));
@@ -1020,6 +1024,7 @@ void diff_layout(int32_t n, int64_t nnz, int32_t n_groups, char* base, feab_diff
     D->tcol = reinterpret_cast<int32_t*>(tc);
     D->vhi = reinterpret_cast<uint32_t*>(hi);
     D->vlo = reinterpret_cast<uint16_t*>(lo);
+    D->vlo2 = reinterpret_cast<uint8_t*>(lo2);
     D->gmask = reinterpret_cast<uint8_t*>(gm);
     D->S = reinterpret_cast<double*>(ss);
     D->goff = reinterpret_cast<int32_t*>(go);
@@ -1068,7 +1073,7 @@ extern "C" int32_t feab_diff_operator_build(const feab_csr* M, const int32_t* do
   FEAB_CUDA(scan_exclusive_i32(out->voff, out->voff, G, X.scan, X.total, s));
   const int wpb = kThreads / 32;
   k_build_diff<<<(G + wpb - 1) / wpb, kThreads, 0, s>>>(G, M->group_ptr, M->row_ptr, M->col_idx, M->vals64, dof_of,
-                                                         out->goff, out->voff, out->tcol, out->vhi, out->vlo,
+                                                         out->goff, out->voff, out->tcol, out->vhi, out->vlo, out->vlo2,
                                                          out->gmask, out->S, X.err);
   count_launches(1);
   FEAB_CHECK_LAUNCH();

@@ -42,7 +42,7 @@ class CSR(C.Structure):
 
 class DiffOperator(C.Structure):
     _fields_ = [("tcol", C.c_void_p), ("vhi", C.c_void_p), ("vlo", C.c_void_p), ("gmask", C.c_void_p),
-                ("S", C.c_void_p), ("goff", C.c_void_p), ("voff", C.c_void_p)]
+                ("S", C.c_void_p), ("goff", C.c_void_p), ("voff", C.c_void_p), ("vlo2", C.c_void_p)]
 
 
 class SellOperator(C.Structure):

@@ -81,7 +81,8 @@ class ReducedOperator:
     _sell: dict = None
 
     def diff_operator(self):
-        """The 48-bit difference-form operator (feab_diff_operator_build), cached."""
+        """The difference-form operator of the mixed block-PCG (7-byte values, 44-bit mantissas;
+        feab_diff_operator_build), cached."""
         if self._diff is None:
             p = self.pattern
             if p.group_ptr is None or p.free_map.numel() == 0:

@@ -71,13 +71,17 @@ typedef struct feab_csr {
 
 /* Difference-form operator built from the FP64 CSR by feab_diff_operator_build (storage is
  * caller memory, feab_diff_operator_bytes).  Applies y_a = sum_{b!=a} K_ab (x_b - x_a) + S_a x_a
- * with K_ab rounded to 36 mantissa bits (6 bytes each) and S_a = sum_b K_ab accumulated in FP64,
+ * with K_ab rounded to 44 mantissa bits (7 bytes each: vhi, vlo, vlo2) and S_a = sum_b K_ab
+ * accumulated in FP64,
  * evaluated as sum_{b!=a} K_ab x_b + T_a x_a with T_a = S_a - W_a, W_a = sum_{b!=a} K_ab over the
  * rounded values: the same value, so the same rounding error; S holds T.
  * Layout per node row group g (the f rows of one node): its off-node columns, padded to a
  * multiple of 4 (Lp_g), start at goff[g] in tcol; its values start at voff[g], row-major
- * (f rows x Lp_g), so every 4-column quad is one 16-byte (vhi) + 8-byte (vlo) load.  Padding
- * columns point at the node's own first free DOF with value 0. */
+ * (f rows x Lp_g), so every 4-column quad is one 16-byte (vhi) + 8-byte (vlo) + 4-byte (vlo2)
+ * load.  Padding columns point at the node's own first free DOF with value 0.  (44 bits keep the
+ * operator's FP64 residual floor far below 1e-9 on every mesh tried, so the mixed block-PCG
+ * keeps FP64's iteration count; 36 bits, the single-right-hand-side sliced operator's width,
+ * leave it above 1e-9 on some meshes and moduli.) */
 typedef struct feab_diff_operator {
   int32_t* tcol;     /* sum Lp_g: column | (DOF component << 30)            */
   uint32_t* vhi;     /* sum f_g Lp_g: upper 32 bits of the rounded double   */
@@ -86,6 +90,7 @@ typedef struct feab_diff_operator {
   double* S;         /* 3 n: own-node terms T = S - W per DOF component      */
   int32_t* goff;     /* n_groups + 1: first tagged column of each group     */
   int32_t* voff;     /* n_groups + 1: first value of each group             */
+  uint8_t* vlo2;     /* sum f_g Lp_g: the 8 bits below vlo                  */
 } feab_diff_operator;
 
 /* Sliced (SELL-32) node-group operator for the single-right-hand-side PCG, built from the CSR

@@ -49,7 +49,7 @@ def parse():
                     help="skip the oracle job (CPU baseline and the full-size accuracy check against the oracle)")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery",
-                                           "simp_oc", "elements", "modal"],
+                                           "simp_oc", "elements", "modal", "block_step"],
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
@@ -976,6 +976,68 @@ def workload_modal(args):
                                        "64x16x16 mesh takes about a minute on 8 cores"}}
 
 
+def workload_block_step(args):
+    """The block-PCG step on the 128x32x32 cantilever with a 64-column panel of seeded random
+    right-hand sides (the snapshot case's width), FP64 and mixed: the time of one step (three
+    kernels) from CUDA events over runs of 4 and 4 + 8 * steps steps at tol 0 (no column
+    converges; the difference removes setup and capture), at the tuned launch shape; and the
+    block SpMM alone (feab_block_spmm, the same group SpMM code as the step's kernel A) with L2
+    flushed before each launch, against the algorithmic bytes of one block SpMM:
+    nnz * (8 + 4) + 4 (n + 1) + 2 n k * 8."""
+    import torch
+    from feab200 import cantilever
+    from feab200.batched import ProblemBatch, block_pcg, tuned_block_shape
+    from feab200.panel import block_spmm
+    c = cantilever.random_tip_cantilever(*args.shape)
+    b = ProblemBatch([(c.mesh.nodes, c.mesh.elements, c.D, c.fixed, c.F)])
+    op = b.assemble()
+    k = 64
+    B = torch.as_tensor(np.random.default_rng(0).standard_normal((op.n, k))).cuda()
+    long = 4 + 8 * max(1, args.steps)
+    out = {}
+    for prec in ("fp64", "mixed"):
+        shape = tuned_block_shape(op, b.row_bounds, B, [k], prec)
+
+        def run(m):
+            a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record()
+            block_pcg(op, b.row_bounds, B, [k], tol=0.0, maxiter=m, precision=prec, max_groups=shape.item_groups,
+                      tile_width=shape.tile_width, tune=False)
+            e.record()
+            e.synchronize()
+            return a.elapsed_time(e)
+        for _ in range(max(1, args.warmup)):
+            run(4)
+        t4, tl = min(run(4) for _ in range(2)), min(run(long) for _ in range(2))
+        out[prec] = {"us_per_step": round((tl - t4) * 1e3 / (long - 4), 1), "item_groups": shape.item_groups,
+                     "tile_width": shape.tile_width}
+    flush = L2Flush(op.vals64.device)
+    Y = torch.empty_like(B)
+    block_spmm(op, B, out=Y)
+    times = []
+    for _ in range(max(3, args.steps)):
+        flush()
+        a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        block_spmm(op, B, out=Y)
+        e.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(e) * 1e-3)
+    t = statistics.mean(times)
+    nbytes = op.nnz * 12 + 4 * (op.n + 1) + 2 * op.n * k * 8
+    flops = 2 * op.nnz * k
+    peak, kind = measured_peak()
+    return {"metric": f"block-PCG step time, {'x'.join(map(str, args.shape))} cantilever, 64 right-hand sides",
+            "value": out["fp64"]["us_per_step"], "unit": "us", "steps_timed": long - 4, "step": out,
+            "mixed_speedup_vs_fp64": round(out["fp64"]["us_per_step"] / out["mixed"]["us_per_step"], 3),
+            "block_spmm": {"us": round(t * 1e6, 1), "bytes": int(nbytes), "fp64_gflop": round(flops / 1e9, 2),
+                           "roofline": {"bound": "hbm", "achieved": round(nbytes / t / 1e9, 1), "peak": peak,
+                                        "unit": "GB/s", "frac": round(nbytes / t / 1e9 / peak, 3),
+                                        "peak_source": f"MEASURED_PEAKS.json hbm_gbs (of {kind})"},
+                           "fp64_tflops": round(flops / t / 1e12, 2)},
+            "timing": "step: CUDA events over whole runs; SpMM: CUDA events around each launch, L2 flushed before each"}
+
+
 class _NoCheck:
     """A device status that is never read back, so a timed element-matrix launch has no sync."""
 
@@ -1071,7 +1133,8 @@ def main():
     if args.workload != "cantilever":
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
               "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery,
-              "simp_oc": workload_simp_oc, "elements": workload_elements, "modal": workload_modal}[args.workload]
+              "simp_oc": workload_simp_oc, "elements": workload_elements, "modal": workload_modal,
+              "block_step": workload_block_step}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})

@@ -385,16 +385,26 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
   const int64_t row0 = c0 * kChunk, row1 = min64(n, c1 * kChunk);
 
   // per-column exponents over this CTA's rows: thread t reads 4 columns (float4) of rows
-  // row0 + t / 16, + 16, ...
+  // row0 + t / 16, + 16, ..., kI8Ahead rows in flight per thread
   {
+    constexpr int kI8Ahead = 16;
+    constexpr int kRowStep = kI8Threads / 16;
     float mx[4] = {0.f, 0.f, 0.f, 0.f};
     const int cq = (tid & 15) * 4;
-    for (int64_t r = row0 + (tid >> 4); r < row1; r += kI8Threads / 16) {
-      const float4 v = __ldg(reinterpret_cast<const float4*>(X + r * kCols + cq));
-      mx[0] = fmaxf(mx[0], fabsf(v.x));
-      mx[1] = fmaxf(mx[1], fabsf(v.y));
-      mx[2] = fmaxf(mx[2], fabsf(v.z));
-      mx[3] = fmaxf(mx[3], fabsf(v.w));
+    for (int64_t r = row0 + (tid >> 4); r < row1; r += kRowStep * kI8Ahead) {
+      float4 v[kI8Ahead];
+#pragma unroll
+      for (int u = 0; u < kI8Ahead; ++u) {
+        const int64_t rr = r + (int64_t)kRowStep * u;
+        v[u] = rr < row1 ? __ldg(reinterpret_cast<const float4*>(X + rr * kCols + cq)) : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < kI8Ahead; ++u) {
+        mx[0] = fmaxf(mx[0], fabsf(v[u].x));
+        mx[1] = fmaxf(mx[1], fabsf(v[u].y));
+        mx[2] = fmaxf(mx[2], fabsf(v[u].z));
+        mx[3] = fmaxf(mx[3], fabsf(v[u].w));
+      }
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) S.colmax[tid >> 4][cq + j] = mx[j];

@@ -4,9 +4,11 @@
 _select_rank pod.py:163-176).  The FP64 economy SVD of the reference (pod.py:140-147) is
 replaced by the method of snapshots: the 64 x 64 Gram matrix X^T X, its FP64 eigenvalues by a
 one-CTA Jacobi solver (feab_symeig_jacobi), singular values sqrt(lambda), and modes
-U = X V / sigma.  Three Gram kernels:
+U = X V / sigma.  Three Gram kernels; the default ``gram="auto"`` takes the int8 one for FP32
+snapshots and the FP64 one for FP64 snapshots (whose values carry more bits than seven 7-bit
+digits keep):
 
-* ``gram="int8"`` (default): the tensor cores with exact products (seven signed 7-bit digits per
+* ``gram="int8"``: the tensor cores with exact products (seven signed 7-bit digits per
   value, tcgen05.mma kind::i8 with int32 accumulation, FP64 combination; feab_gram_int8) --
   FP64-level accuracy at tensor-core speed; at 1,382,976 x 64 its singular values agree with the
   FP64 Gram's to 1.4e-9 and it runs in 0.81 ms against 1.2 ms;
@@ -133,7 +135,7 @@ class PodBasis:
         self.mass_weighted = False
         self.M = None
 
-    def fit(self, snapshots, n_modes=None, energy_threshold=None, M=None, device=None, gram="int8"):
+    def fit(self, snapshots, n_modes=None, energy_threshold=None, M=None, device=None, gram="auto"):
         if n_modes is None and energy_threshold is None:
             raise ValueError("fit() needs at least one of n_modes, energy_threshold")
         if M is not None:
@@ -145,8 +147,10 @@ class PodBasis:
         n, k = X.shape
         if k > MAX_SNAPSHOTS:
             raise NotImplementedError(f"PodBasis.fit: at most {MAX_SNAPSHOTS} snapshots per panel on the GPU path")
-        if gram not in ("fp64", "bf16x3", "int8"):
-            raise ValueError("gram must be 'fp64', 'bf16x3' or 'int8'")
+        if gram not in ("auto", "fp64", "bf16x3", "int8"):
+            raise ValueError("gram must be 'auto', 'fp64', 'bf16x3' or 'int8'")
+        if gram == "auto":
+            gram = "int8" if X.dtype == torch.float32 else "fp64"
         dt = torch.float64 if gram == "fp64" else torch.float32
         Xp = torch.zeros((n, MAX_SNAPSHOTS), dtype=dt, device=dev)
         Xp[:, :k] = X.to(dt)

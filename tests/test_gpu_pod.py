@@ -137,3 +137,22 @@ def test_pod_int8_gram_matches_the_fp64_svd_on_a_decaying_spectrum():
     err = {g: np.abs(v - ref) / ref for g, v in got.items()}
     assert err["int8"].max() < 1e-7, err
     assert err["int8"].max() <= 10 * err["fp64"].max() + 1e-12
+
+
+def test_pod_auto_gram_picks_by_input_precision():
+    """FP32 snapshots go to the exact-product tensor-core Gram, FP64 snapshots to the FP64 Gram
+    (their values carry more bits than the seven 7-bit digits keep); both agree with the FP64
+    SVD of their own input."""
+    from feab200.pod import PodBasis
+    rng = np.random.default_rng(12)
+    n = 50_000
+    U, _ = np.linalg.qr(rng.standard_normal((n, 12)))
+    X = (U * np.logspace(0, -4, 12)) @ np.linalg.qr(rng.standard_normal((12, 12)))[0]
+    for dt in (np.float32, np.float64):
+        Xd = X.astype(dt)
+        ref = np.linalg.svd(Xd.astype(np.float64), compute_uv=False)[:8]
+        s_auto = PodBasis().fit(torch.as_tensor(Xd).cuda(), n_modes=8).singular_values[:8]
+        s_same = PodBasis().fit(torch.as_tensor(Xd).cuda(), n_modes=8,
+                                gram="int8" if dt == np.float32 else "fp64").singular_values[:8]
+        assert np.array_equal(s_auto, s_same)
+        assert (np.abs(s_auto - ref) / ref).max() < 1e-7

@@ -34,14 +34,14 @@
 #include "feab_sell.cuh"
 
 namespace feab {
-// 1: the sliced path's step kernels (P, A, B) are launched with programmatic dependent launch
+// 1 (default): the sliced path's step kernels (P, A, B) are launched with programmatic dependent launch
 // inside the captured chunk: each kernel lets its successor's CTAs launch as soon as all of its
 // own CTAs are running, and every kernel waits (griddepcontrol.wait) for its predecessor's
 // completion and memory before it reads anything, so the launch latency of a kernel boundary
 // overlaps the tail of the previous kernel.  Without the launch attribute the two instructions
-// are no-ops.
+// are no-ops.  Measured at 128x32x32: 62.4 -> 62.0 us per FP64 iteration, 54.6 -> 54.0 mixed.
 #ifndef FEAB_PDL
-#define FEAB_PDL 0
+#define FEAB_PDL 1
 #endif
 __device__ __forceinline__ void pdl_enter() {
 #if FEAB_PDL

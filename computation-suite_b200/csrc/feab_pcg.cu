@@ -34,21 +34,6 @@
 #include "feab_sell.cuh"
 
 namespace feab {
-// 1 (default): the sliced path's step kernels (P, A, B) are launched with programmatic dependent launch
-// inside the captured chunk: each kernel lets its successor's CTAs launch as soon as all of its
-// own CTAs are running, and every kernel waits (griddepcontrol.wait) for its predecessor's
-// completion and memory before it reads anything, so the launch latency of a kernel boundary
-// overlaps the tail of the previous kernel.  Without the launch attribute the two instructions
-// are no-ops.  Measured at 128x32x32: 62.4 -> 62.0 us per FP64 iteration, 54.6 -> 54.0 mixed.
-#ifndef FEAB_PDL
-#define FEAB_PDL 1
-#endif
-__device__ __forceinline__ void pdl_enter() {
-#if FEAB_PDL
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-  asm volatile("griddepcontrol.wait;" ::: "memory");
-#endif
-}
 namespace {
 
 constexpr int kThreads = 256;
@@ -403,7 +388,6 @@ __global__ void __launch_bounds__(kThreads, 4) k_step_a(PcgArgs A) {
 
 // Sliced path, kernel P: p = z + beta p in place when a new direction is pending.
 __global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
-  pdl_enter();
   const PcgState* S = A.S_;
   if (S->done || !S->p_pending) return;
   const double beta = S->beta;
@@ -425,7 +409,6 @@ __global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
 // mixed reliable step, the FP64 residual r = b - K64 x through the CSR values instead.
 template <int PREC>
 __global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step_a_sell(PcgArgs A) {
-  pdl_enter();
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
@@ -506,7 +489,6 @@ __global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step
 // Step kernel B.
 template <int PREC>
 __global__ void __launch_bounds__(kThreads) k_step_b(PcgArgs A) {
-  pdl_enter();
   PcgState* S = A.S_;
   if (S->done) return;
   const int mode = S->mode;
@@ -850,29 +832,9 @@ int sell_grid(const PcgArgs& A) {
 
 template <int PREC>
 void launch_step_sell(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
-#if FEAB_PDL
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  attr[0].val.programmaticStreamSerializationAllowed = 1;
-  cudaLaunchConfig_t cfg = {};
-  cfg.blockDim = dim3(kThreads);
-  cfg.dynamicSmemBytes = 0;
-  cfg.stream = s;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  if (!FEAB_SELL_FUSED_P) {
-    cfg.gridDim = dim3(gr.b);
-    cudaLaunchKernelEx(&cfg, k_step_p, A);
-  }
-  cfg.gridDim = dim3(sell_grid(A));
-  cudaLaunchKernelEx(&cfg, k_step_a_sell<PREC>, A);
-  cfg.gridDim = dim3(gr.b);
-  cudaLaunchKernelEx(&cfg, k_step_b<PREC>, A);
-#else
   if (!FEAB_SELL_FUSED_P) k_step_p<<<gr.b, kThreads, 0, s>>>(A);
   k_step_a_sell<PREC><<<sell_grid(A), kThreads, 0, s>>>(A);
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
-#endif
 }
 
 int normalize_lpg(int lpg) { return lpg == 4 || lpg == 8 || lpg == 16 || lpg == 32 ? lpg : 16; }

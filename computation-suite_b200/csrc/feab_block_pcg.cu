@@ -95,7 +95,7 @@ __device__ __forceinline__ bool last_of_problem(uint32_t* ticket, int n_items_p,
 // one contiguous row range (the items of a problem cover consecutive row groups), which cuts
 // their per-item block reductions and tickets; the SpMM keeps the finer items for its balance.
 #ifndef FEAB_BLOCK_BRUN
-#define FEAB_BLOCK_BRUN 1
+#define FEAB_BLOCK_BRUN 4
 #endif
 constexpr int kBRun = FEAB_BLOCK_BRUN;
 
@@ -136,8 +136,13 @@ constexpr int kUnroll = FEAB_BLOCK_UNROLL;
 constexpr int kVecU = FEAB_BLOCK_VECU;
 // minimum resident CTAs per SM of the SpMM kernel (register budget)
 #ifndef FEAB_BLOCK_MINB
-#define FEAB_BLOCK_MINB 1
+#define FEAB_BLOCK_MINB 2
 #endif
+// gathers in flight per lane in the FP64 SpMM (the mixed one keeps kUnroll: at 16 its decode and
+// own-node term push it past the 128 registers of two CTAs per SM); measured at 128x32x32 with
+// 64 columns: 1078 -> 1003 us per FP64 step
+constexpr int kUnrollFp64 = 16;
+static_assert(kStageCols % kUnrollFp64 == 0 && kStageCols % kUnroll == 0, "vector reads stay inside the stage");
 
 struct __align__(16) GroupStage {
   int col[kStageCols];
@@ -172,7 +177,7 @@ __device__ __forceinline__ void gather_row(const double* __restrict__ src, int j
 // SpMM for one row group: acc[row][q] = (K src)[row][panel_col(cl, q)].
 // Lanes are split into MPW = max(1, 32/K) sub-warps, each walking every MPW-th matrix column;
 // a lane covers CPL = max(1, K/32) panel columns.
-template <int K, bool DIFF>
+template <int K, bool DIFF, int U = kUnroll>
 __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, GroupStage& st,
                                            const double* __restrict__ src,
                                            double (&acc)[3][K >= 32 ? K / 32 : 1]) {
@@ -237,14 +242,14 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
       }
     }
     __syncwarp();
-    if constexpr (MPW == 1 && FEAB_BLOCK_VLDS && kUnroll % 4 == 0) {
-      // m0 is a multiple of kUnroll, so the vector reads stay inside the kStageCols-entry stage
+    if constexpr (MPW == 1 && FEAB_BLOCK_VLDS && U % 4 == 0) {
+      // m0 is a multiple of U, so the vector reads stay inside the kStageCols-entry stage
       // (entries past nc are read but not used)
-      for (int m0 = 0; m0 < nc; m0 += kUnroll) {
-        unsigned t[kUnroll];
-        double xv[kUnroll][CPL];
+      for (int m0 = 0; m0 < nc; m0 += U) {
+        unsigned t[U];
+        double xv[U][CPL];
 #pragma unroll
-        for (int u4 = 0; u4 < kUnroll / 4; ++u4) {
+        for (int u4 = 0; u4 < U / 4; ++u4) {
           const int4 tq = *reinterpret_cast<const int4*>(&st.col[m0 + 4 * u4]);
           t[4 * u4] = (unsigned)tq.x;
           t[4 * u4 + 1] = (unsigned)tq.y;
@@ -252,7 +257,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
           t[4 * u4 + 3] = (unsigned)tq.w;
         }
 #pragma unroll
-        for (int u = 0; u < kUnroll; ++u) {
+        for (int u = 0; u < U; ++u) {
           if (m0 + u < nc) {
             gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), cl, xv[u]);
           } else {
@@ -261,7 +266,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
           }
         }
 #pragma unroll
-        for (int u2 = 0; u2 < kUnroll / 2; ++u2) {
+        for (int u2 = 0; u2 < U / 2; ++u2) {
           if (m0 + 2 * u2 >= nc) break;
           const double2 w0 = *reinterpret_cast<const double2*>(&st.val[0][m0 + 2 * u2]);
           const double2 w1 = *reinterpret_cast<const double2*>(&st.val[1][m0 + 2 * u2]);
@@ -287,11 +292,11 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
         }
       }
     } else
-    for (int m0 = sub; m0 < nc; m0 += MPW * kUnroll) {
-      unsigned t[kUnroll];
-      double xv[kUnroll][CPL];
+    for (int m0 = sub; m0 < nc; m0 += MPW * U) {
+      unsigned t[U];
+      double xv[U][CPL];
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
+      for (int u = 0; u < U; ++u) {
         const int m = m0 + u * MPW;
         t[u] = m < nc ? (unsigned)st.col[m] : 0u;
         if (m < nc) {
@@ -302,7 +307,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
         }
       }
 #pragma unroll
-      for (int u = 0; u < kUnroll; ++u) {
+      for (int u = 0; u < U; ++u) {
         const int m = m0 + u * MPW;
         if (m >= nc) break;
         const double w0 = st.val[0][m], w1 = st.val[1][m], w2 = st.val[2][m];
@@ -630,7 +635,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
         if (!diff) group_spmm<K, false>(A, g, lane, stage[w], src, acc);
         else group_spmm<K, true>(A, g, lane, stage[w], po, acc);
       } else {
-        group_spmm<K, false>(A, g, lane, stage[w], po, acc);
+        group_spmm<K, false, kUnrollFp64>(A, g, lane, stage[w], po, acc);
       }
       if (lane < LW) {
         const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
@@ -762,7 +767,7 @@ __global__ void __launch_bounds__(kThreads) k_bstep_p(BArgs A) {
 // Step B: X += alpha P, R -= alpha AP (CG step; a reliable step leaves both); per column r.r
 // and r.z with z = M r formed on the fly; per-column convergence, beta, problem bookkeeping.
 #ifndef FEAB_BLOCK_B_MINB
-#define FEAB_BLOCK_B_MINB 1
+#define FEAB_BLOCK_B_MINB 2
 #endif
 template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A) {
@@ -975,7 +980,7 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_block_spmm(BArgs 
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int g = blockIdx.x * kWarps + w; g < A.n_groups; g += gridDim.x * kWarps) {
     double acc[3][CPL];
-    group_spmm<K, false>(A, g, lane, stage[w], src, acc);
+    group_spmm<K, false, kUnrollFp64>(A, g, lane, stage[w], src, acc);
     if (lane < LW) {
       const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
 #pragma unroll

@@ -301,10 +301,13 @@ __global__ void __launch_bounds__(kThreadsG) k_gram_bf16x3(const float* __restri
 // S_(a+1)^T S_c (weight a + c + 1) to the bottom 64 of region R_(a+c).  Seven regions
 // R_2..R_8 of 64 columns each (448 of TMEM's 512) hold every needed pair with a fixed weight
 // per half: weight v on top of R_v, v + 1 on the bottom.  16 MMAs (32 instructions) per chunk.
-// The int32 regions are drained into FP64 registers every kI8Drain chunks (and at the end),
-// which bounds them below 2^31.  Per-CTA FP64 partials are summed by k_gram_reduce (fixed order).
+// The int32 regions are drained every kI8Drain chunks (and at the end) into an FP64 accumulator in
+// shared memory, which bounds them below 2^31; per-CTA FP64 partials are summed by k_gram_reduce
+// (fixed order).  512 threads: the digits are formed with integer operations from the FP32 bit
+// pattern (a 49-bit fixed-point magnitude, then 7-bit fields), and the drain keeps 16 doubles per
+// thread, so the kernel stays within 128 registers.
 constexpr int kSlices = 7;
-constexpr int kI8Threads = 256;
+constexpr int kI8Threads = 512;
 constexpr int kI8Drain = 192;                        // chunks between drains: < 2^31 / (4 * 64 * 127^2)
 constexpr uint32_t kI8LBO = 128;                     // next core matrix (16 K-bytes) along K
 constexpr uint32_t kI8SBO = 4 * 128;                 // next 8-row group along M / N
@@ -312,8 +315,9 @@ constexpr int kI8SliceBytes = 64 * kChunk;           // one 64-row x 64-K int8 s
 constexpr int kI8Regions = kSlices;                  // R_2 .. R_8
 
 struct __align__(1024) Int8Smem {
-  float stage[kStages][kChunk * kCols];              // 64 KB; reused for the final row exchange
+  float stage[kStages][kChunk * kCols];              // 64 KB
   int8_t tile[2][(kSlices + 1) * kI8SliceBytes];     // 2 x 32 KB; slice 8 stays zero
+  double acc[128 * kCols];                           // 64 KB: the drained sums, one row per TMEM lane
   unsigned long long full_bar[kStages];
   unsigned long long mma_bar[2];
   float colmax[kI8Threads / 16][kCols];
@@ -345,32 +349,56 @@ __device__ __forceinline__ void mma_i8(uint32_t tmem_d, uint64_t da, uint64_t db
       : "memory");
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, int32_t (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = (int32_t)r[i];
+}
+
+// The 7-bit digit fields of |x| 2^(49 - e) (|x| < 2^e), from the FP32 bit pattern: mantissa with
+// its hidden bit, shifted into a 49-bit fixed-point magnitude (bits below 2^(e - 49) drop, the
+// truncation of x = 2^e sum_a s_a 2^(-7a)), then digit a = bits 49 - 7a .. 55 - 7a, with x's sign.
+__device__ __forceinline__ void digits_i8(float x, int e, uint32_t (&d)[kSlices]) {
+  const uint32_t u = __float_as_uint(x);
+  const uint32_t ex = (u >> 23) & 0xffu;
+  const uint64_t mant = (uint64_t)((u & 0x7fffffu) | (ex ? 0x800000u : 0u));
+  const int sh = (ex ? (int)ex : 1) - 101 - e;   // x = mant 2^(ex - 150); 2^(49 - e) more
+  const uint64_t mag = sh >= 0 ? (mant << sh) : (sh > -64 ? (mant >> -sh) : 0ull);
+  const bool neg = (u >> 31) != 0;
+#pragma unroll
+  for (int a = 0; a < kSlices; ++a) {
+    const uint32_t f = (uint32_t)(mag >> (49 - 7 * (a + 1))) & 0x7fu;
+    d[a] = (neg ? (0u - f) : f) & 0xffu;
+  }
+}
+
 // Split the staged FP32 rows of one chunk into the kSlices int8 digit tiles.  Thread t owns
-// column m = t % 64 and rows 16 (t / 64) .. +15 (one 16-byte core-matrix row per digit).
+// column m = t % 64 and rows 8 (t / 64) .. +7 (half of a 16-byte core-matrix row per digit).
 __device__ __forceinline__ void split_chunk_i8(const float* st, int8_t* tiles, int rows, const int* expo) {
   const int m = threadIdx.x & 63, kg = threadIdx.x >> 6;
   const int e = expo[m];
-  int32_t packed[kSlices][4];
+  uint32_t packed[kSlices][2];
 #pragma unroll
-  for (int a = 0; a < kSlices; ++a)
+  for (int a = 0; a < kSlices; ++a) packed[a][0] = packed[a][1] = 0u;
 #pragma unroll
-    for (int w = 0; w < 4; ++w) packed[a][w] = 0;
+  for (int u = 0; u < 8; ++u) {
+    const int k = kg * 8 + u;
+    uint32_t d[kSlices];
+    digits_i8(k < rows ? st[k * kCols + m] : 0.0f, e, d);
 #pragma unroll
-  for (int u = 0; u < 16; ++u) {
-    const int k = kg * 16 + u;
-    float y = k < rows ? ldexpf(st[k * kCols + m], 7 - e) : 0.0f;  // |y| < 128
-#pragma unroll
-    for (int a = 0; a < kSlices; ++a) {
-      const float d = truncf(y);
-      y = (y - d) * 128.0f;
-      packed[a][u >> 2] |= (int32_t)(((uint32_t)(int32_t)d & 0xffu) << (8 * (u & 3)));
-    }
+    for (int a = 0; a < kSlices; ++a) packed[a][u >> 2] |= d[a] << (8 * (u & 3));
   }
-  const uint32_t off = (m / 8) * kI8SBO + kg * kI8LBO + (m % 8) * 16;
+  const uint32_t off = (m / 8) * kI8SBO + (kg >> 1) * kI8LBO + (m % 8) * 16 + (kg & 1) * 8;
 #pragma unroll
   for (int a = 0; a < kSlices; ++a)
-    *reinterpret_cast<int4*>(tiles + a * kI8SliceBytes + off) =
-        make_int4(packed[a][0], packed[a][1], packed[a][2], packed[a][3]);
+    *reinterpret_cast<uint2*>(tiles + a * kI8SliceBytes + off) = make_uint2(packed[a][0], packed[a][1]);
 }
 
 __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __restrict__ X, int64_t n,
@@ -385,9 +413,9 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
   const int64_t row0 = c0 * kChunk, row1 = min64(n, c1 * kChunk);
 
   // per-column exponents over this CTA's rows: thread t reads 4 columns (float4) of rows
-  // row0 + t / 16, + 16, ..., kI8Ahead rows in flight per thread
+  // row0 + t / 16, + 32, ..., kI8Ahead rows in flight per thread
   {
-    constexpr int kI8Ahead = 16;
+    constexpr int kI8Ahead = 8;
     constexpr int kRowStep = kI8Threads / 16;
     float mx[4] = {0.f, 0.f, 0.f, 0.f};
     const int cq = (tid & 15) * 4;
@@ -409,9 +437,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
 #pragma unroll
     for (int j = 0; j < 4; ++j) S.colmax[tid >> 4][cq + j] = mx[j];
   }
-  // zero both tile buffers (the eighth digit tile must stay zero)
+  // zero both tile buffers (the eighth digit tile must stay zero) and the accumulator
   for (int i = tid; i < 2 * (kSlices + 1) * kI8SliceBytes / 16; i += kI8Threads)
     reinterpret_cast<int4*>(&S.tile[0][0])[i] = make_int4(0, 0, 0, 0);
+  for (int i = tid; i < 128 * kCols; i += kI8Threads) S.acc[i] = 0.0;
   if (tid == 0) {
     for (int s = 0; s < kStages; ++s) mbar_init(&S.full_bar[s], 1);
     mbar_init(&S.mma_bar[0], 1);
@@ -446,13 +475,10 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
     }
   }
 
-  // thread t drains TMEM lane 32 (warp % 4) + lane, regions [rbeg, rend): warps 0-3 take
-  // R_2..R_5, warps 4-7 R_6..R_8
+  // the drain: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its lane quarter) and columns
+  // 16 (w / 4) .. + 15 of every region, and adds them, weighted, into row lane_row of S.acc
   const int lane_row = 32 * (warp & 3) + lane;
-  const int rbeg = warp < 4 ? 0 : 4, rend = warp < 4 ? 4 : kI8Regions;
-  double acc[kCols];
-#pragma unroll
-  for (int j = 0; j < kCols; ++j) acc[j] = 0.0;
+  const int col0 = 16 * (warp >> 2);
   bool ok = true;
   int since_drain = 0;
   int64_t issued = 0;
@@ -468,16 +494,18 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
     // top lanes hold weight v of R_v, bottom lanes weight v + 1
     const int wshift = lane_row < 64 ? 0 : 1;
-    for (int r = rbeg; r < rend; ++r) {
+    double sum[16];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) sum[i] = 0.0;
+    for (int r = 0; r < kI8Regions; ++r) {
       const double scale = ldexp(1.0, -7 * (r + 2 + wshift));
+      int32_t v[16];
+      tmem_ld16(tmem + lane_base + (uint32_t)(r * 64 + col0), v);
 #pragma unroll
-      for (int h = 0; h < 2; ++h) {
-        float v[32];
-        tmem_ld32(tmem + lane_base + (uint32_t)(r * 64 + h * 32), v);
-#pragma unroll
-        for (int i = 0; i < 32; ++i) acc[h * 32 + i] += (double)__float_as_int(v[i]) * scale;
-      }
+      for (int i = 0; i < 16; ++i) sum[i] += (double)v[i] * scale;
     }
+#pragma unroll
+    for (int i = 0; i < 16; ++i) S.acc[lane_row * kCols + col0 + i] += sum[i];
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   };
 
@@ -528,7 +556,7 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
   }
   if (!ok) {
     // bounded waits for what is still in flight before TMEM and shared memory are left: the
-    // MMAs of the last issued chunk and the bulk copies of chunks issued - 1 + 1 .. loaded - 1
+    // MMAs of the last issued chunk and the bulk copies of chunks issued .. loaded - 1
     const long long t0 = clock64();
     if (issued > 0) {
       const int64_t last = issued - 1;
@@ -544,21 +572,11 @@ __global__ void __launch_bounds__(kI8Threads, 1) k_gram_int8(const float* __rest
   if (warp == 0) {
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(512) : "memory");
   }
-  // warps 4-7 hand their sums to warps 0-3 (same TMEM rows) through the staging area, then the
-  // partial row lane_row (top: column lane_row of X, bottom: column lane_row - 64), scaled by
-  // 2^(e_i + e_j), goes to part[cta][lane_row][j]
-  double* xch = reinterpret_cast<double*>(&S.stage[0][0]);  // 128 x 64 doubles = 64 KB
-  if (warp >= 4) {
-#pragma unroll
-    for (int j = 0; j < kCols; ++j) xch[lane_row * kCols + j] = acc[j];
-  }
-  __syncthreads();
-  if (warp < 4) {
-    const int ci = lane_row & 63;
-    const int ei = S.expo[ci];
-    double* out = part + ((int64_t)blockIdx.x * 128 + lane_row) * kCols;
-#pragma unroll
-    for (int j = 0; j < kCols; ++j) out[j] = ldexp(acc[j] + xch[lane_row * kCols + j], ei + S.expo[j]);
+  // row r of the partial (top: column r of X, bottom: column r - 64), scaled by 2^(e_i + e_j)
+  double* out = part + (int64_t)blockIdx.x * 128 * kCols;
+  for (int e = tid; e < 128 * kCols; e += kI8Threads) {
+    const int r = e / kCols, j = e % kCols;
+    out[e] = ldexp(S.acc[e], S.expo[r & 63] + S.expo[j]);
   }
 }
 

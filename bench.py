@@ -239,7 +239,8 @@ def e2e_steps(c, precision, tol, steps, warmup):
 def spmv_bytes(op, precision):
     """Algorithmic bytes of one launch of the PCG's SpMV kernel for `precision`, counted from
     what the kernel must read and write once: values, column indices (one row per node
-    group, since the rows of a node share them), row/group pointers, the x vector and y."""
+    group, since the rows of a node share them; 2 bytes each when the sliced operator holds
+    16-bit offsets), row/group pointers, the x vector and y."""
     p = op.pattern
     rp = p.row_ptr.cpu().numpy().astype(np.int64)
     gp = p.group_ptr.cpu().numpy().astype(np.int64)
@@ -248,12 +249,14 @@ def spmv_bytes(op, precision):
     lead = int(lens.sum())
     n, nnz, G = p.n, p.nnz, p.n_groups
     ptrs = 4 * (n + 1) + 4 * (G + 1)
-    if precision == "fp64":
-        return nnz * 8 + 4 * lead + ptrs + 2 * n * 8
     if precision == "fp32":
         return nnz * 4 + 4 * lead + ptrs + 2 * n * 4
+    # the sliced operator reads 2-byte column offsets when they all fit 16 bits
+    ib = 2 if op.sell_operator(precision).tcol16 else 4
+    if precision == "fp64":
+        return nnz * 8 + ib * lead + ptrs + 2 * n * 8
     own = int((f * f).sum())                                   # own-node block entries are skipped
-    return (nnz - own) * 6 + 4 * (lead - n) + ptrs + G + 24 * n + 2 * n * 8
+    return (nnz - own) * 6 + ib * (lead - n) + ptrs + G + 24 * n + 2 * n * 8
 
 
 def spmv_roofline(op, precision, reps, peak_gbs):

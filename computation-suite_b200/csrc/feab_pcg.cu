@@ -407,7 +407,7 @@ __global__ void __launch_bounds__(kThreads) k_step_p(PcgArgs A) {
 
 // Sliced path, kernel A: Ap = K p and p.Ap through the SELL-32 operator (PREC = its kind); in a
 // mixed reliable step, the FP64 residual r = b - K64 x through the CSR values instead.
-template <int PREC>
+template <int PREC, bool IDX16>
 __global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step_a_sell(PcgArgs A) {
   PcgState* S = A.S_;
   if (S->done) return;
@@ -438,9 +438,9 @@ __global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step
       const SellLane L = sell_lane(A.sell, sl, lane);
       double acc[3], xs[3];
       if (pend)
-        sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc, xs);
+        sell_apply<PREC, IDX16>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.z + j) + beta * __ldg(po + j); }, acc, xs);
       else
-        sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(po + j); }, acc, xs);
+        sell_apply<PREC, IDX16>(A.sell, sl, lane, L, [&](int j) { return __ldg(po + j); }, acc, xs);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         if (k < L.f) {
@@ -457,7 +457,7 @@ __global__ void __launch_bounds__(kThreads, SellTuning<PREC>::kMinBlocks) k_step
     for (int sl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; sl < A.sell.n_slices; sl += nw) {
       const SellLane L = sell_lane(A.sell, sl, lane);
       double acc[3], xs[3];
-      sell_apply<PREC>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.p0 + j); }, acc, xs);
+      sell_apply<PREC, IDX16>(A.sell, sl, lane, L, [&](int j) { return __ldg(A.p0 + j); }, acc, xs);
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
         if (k < L.f) {
@@ -833,7 +833,8 @@ int sell_grid(const PcgArgs& A) {
 template <int PREC>
 void launch_step_sell(const PcgArgs& A, const Grids& gr, cudaStream_t s) {
   if (!FEAB_SELL_FUSED_P) k_step_p<<<gr.b, kThreads, 0, s>>>(A);
-  k_step_a_sell<PREC><<<sell_grid(A), kThreads, 0, s>>>(A);
+  if (A.sell.tcol16) k_step_a_sell<PREC, true><<<sell_grid(A), kThreads, 0, s>>>(A);
+  else k_step_a_sell<PREC, false><<<sell_grid(A), kThreads, 0, s>>>(A);
   k_step_b<PREC><<<gr.b, kThreads, 0, s>>>(A);
 }
 
@@ -950,7 +951,7 @@ void fill_sell(const feab_csr* M, const feab_sell_operator* D, PcgArgs* A) {
 bool sell_fits(const feab_csr* M, const feab_sell_operator* D, int kind) {
   auto al = [](const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; };
   return D && M->group_ptr && M->n_groups > 0 && D->kind == kind && D->n_slices == (M->n_groups + 31) / 32 &&
-         D->soff && D->tcol && al(D->tcol, 16) &&
+         D->soff && D->tcol && al(D->tcol, 16) && (!D->tcol16 || al(D->tcol16, 8)) &&
          (kind == FEAB_PREC_FP64 ? (D->v64 != nullptr && al(D->v64, 16))
                                  : (D->vhi && D->vlo && D->gmask && D->S && al(D->vhi, 16) && al(D->vlo, 8)));
 }

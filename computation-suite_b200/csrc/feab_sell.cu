@@ -17,6 +17,7 @@ struct SellScratch {
   int64_t* scan;
   int64_t* total;
   int32_t* err;
+  int32_t* wide;   // set when a column lies more than 16 bits from its lane's first row
 };
 
 // Storage: soff, scan scratch, flags, then columns and values for n_slices slices of at most
@@ -33,8 +34,9 @@ void sell_layout(int32_t n, int32_t n_groups, int32_t max_row_len, int32_t kind,
   const size_t steps = (size_t)ns * (size_t)round4(max_row_len);
   char* so = take(sizeof(int32_t) * ((size_t)ns + 1));
   char* sc = take(sizeof(int64_t) * ((size_t)scan_blocks((int64_t)ns + 1) + 2));
-  char* tt = take(sizeof(int64_t) + sizeof(int32_t));
+  char* tt = take(sizeof(int64_t) + 2 * sizeof(int32_t));
   char* tc = take(sizeof(int32_t) * 32 * steps);
+  char* t16 = take(sizeof(int16_t) * 32 * steps);
   char *v64 = nullptr, *hi = nullptr, *lo = nullptr, *gm = nullptr, *ss = nullptr;
   if (kind == FEAB_PREC_FP64) {
     v64 = take(sizeof(double) * 96 * steps);
@@ -49,6 +51,7 @@ void sell_layout(int32_t n, int32_t n_groups, int32_t max_row_len, int32_t kind,
     D->n_slices = ns;
     D->soff = reinterpret_cast<int32_t*>(so);
     D->tcol = reinterpret_cast<int32_t*>(tc);
+    D->tcol16 = reinterpret_cast<int16_t*>(t16);
     D->v64 = reinterpret_cast<double*>(v64);
     D->vhi = reinterpret_cast<uint32_t*>(hi);
     D->vlo = reinterpret_cast<uint16_t*>(lo);
@@ -59,6 +62,7 @@ void sell_layout(int32_t n, int32_t n_groups, int32_t max_row_len, int32_t kind,
     X->scan = reinterpret_cast<int64_t*>(sc);
     X->total = reinterpret_cast<int64_t*>(tt);
     X->err = reinterpret_cast<int32_t*>(tt + sizeof(int64_t));
+    X->wide = reinterpret_cast<int32_t*>(tt + sizeof(int64_t) + sizeof(int32_t));
   }
   if (total) *total = off;
 }
@@ -91,6 +95,7 @@ __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_
                                                         const double* __restrict__ vals,
                                                         const int32_t* __restrict__ dof_of,
                                                         const int32_t* __restrict__ soff, int32_t* __restrict__ tcol,
+                                                        int16_t* __restrict__ tcol16, int32_t* __restrict__ wide,
                                                         double* __restrict__ v64, uint32_t* __restrict__ vhi,
                                                         uint16_t* __restrict__ vlo, uint8_t* __restrict__ gmask,
                                                         double* __restrict__ Ssum, int32_t* __restrict__ err) {
@@ -139,6 +144,9 @@ __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_
       tag = diff ? (int32_t)((uint32_t)col | ((uint32_t)(dof_of[col] % 3) << 30)) : col;
     }
     tcol[e] = tag;
+    const int delta = (int)((uint32_t)tag & 0x3fffffffu) - r0;
+    if (delta < -32768 || delta > 32767) atomicExch(wide, 1);
+    tcol16[e] = (int16_t)delta;
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
       const double v = (real && k < f) ? vals[row_ptr[r0 + k] + c] : 0.0;
@@ -175,7 +183,7 @@ __global__ void __launch_bounds__(kThreads) k_sell_fill(int32_t n_groups, int32_
   }
 }
 
-template <int KIND>
+template <int KIND, bool IDX16>
 __global__ void __launch_bounds__(kThreads, SellTuning<KIND>::kMinBlocks) k_sell_spmv(SellView V, const double* __restrict__ x,
                                                            double* __restrict__ y) {
   const int lane = threadIdx.x & 31;
@@ -183,7 +191,7 @@ __global__ void __launch_bounds__(kThreads, SellTuning<KIND>::kMinBlocks) k_sell
   for (int s = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; s < V.n_slices; s += nw) {
     const SellLane L = sell_lane(V, s, lane);
     double acc[3], xs[3];
-    sell_apply<KIND>(V, s, lane, L, [&](int j) { return __ldg(x + j); }, acc, xs);
+    sell_apply<KIND, IDX16>(V, s, lane, L, [&](int j) { return __ldg(x + j); }, acc, xs);
     if (L.f > 0) y[L.r0] = acc[0];
     if (L.f > 1) y[L.r0 + 1] = acc[1];
     if (L.f > 2) y[L.r0 + 2] = acc[2];
@@ -199,6 +207,7 @@ SellView sell_view(const feab_csr* A, const feab_sell_operator* op) {
   V.n_groups = A->n_groups;
   V.soff = op->soff;
   V.tcol = op->tcol;
+  V.tcol16 = op->tcol16;
   V.v64 = op->v64;
   V.vhi = op->vhi;
   V.vlo = op->vlo;
@@ -211,8 +220,13 @@ SellView sell_view(const feab_csr* A, const feab_sell_operator* op) {
 void launch_sell_spmv(const SellView& V, const double* x, double* y, cudaStream_t s) {
   const int wpb = kThreads / 32;
   const int grid = std::max(1, std::min((V.n_slices + wpb - 1) / wpb, sm_count() * 8));
-  if (V.kind == FEAB_PREC_FP64) k_sell_spmv<FEAB_PREC_FP64><<<grid, kThreads, 0, s>>>(V, x, y);
-  else k_sell_spmv<FEAB_PREC_MIXED><<<grid, kThreads, 0, s>>>(V, x, y);
+  if (V.kind == FEAB_PREC_FP64) {
+    if (V.tcol16) k_sell_spmv<FEAB_PREC_FP64, true><<<grid, kThreads, 0, s>>>(V, x, y);
+    else k_sell_spmv<FEAB_PREC_FP64, false><<<grid, kThreads, 0, s>>>(V, x, y);
+  } else {
+    if (V.tcol16) k_sell_spmv<FEAB_PREC_MIXED, true><<<grid, kThreads, 0, s>>>(V, x, y);
+    else k_sell_spmv<FEAB_PREC_MIXED, false><<<grid, kThreads, 0, s>>>(V, x, y);
+  }
   count_launches(1);
 }
 
@@ -244,7 +258,7 @@ extern "C" int32_t feab_sell_operator_build(const feab_csr* A, const int32_t* do
   if (need == 0 || need > storage_bytes) return FEAB_BAD_ARG;
   SellScratch X;
   sell_layout(A->n, A->n_groups, max_row_len, kind, static_cast<char*>(storage), out, &X, nullptr);
-  FEAB_CUDA(cudaMemsetAsync(X.err, 0, sizeof(int32_t), s));
+  FEAB_CUDA(cudaMemsetAsync(X.err, 0, 2 * sizeof(int32_t), s));  // err and wide
   k_sell_widths<<<(ns + kThreads - 1) / kThreads, kThreads, 0, s>>>(A->n_groups, ns, kind, round4(max_row_len),
                                                                      A->group_ptr, A->row_ptr, out->soff, X.err);
   count_launches(1);
@@ -252,14 +266,16 @@ extern "C" int32_t feab_sell_operator_build(const feab_csr* A, const int32_t* do
   FEAB_CUDA(scan_exclusive_i32(out->soff, out->soff, ns, X.scan, X.total, s));
   const int wpb = kThreads / 32;
   k_sell_fill<<<(ns + wpb - 1) / wpb, kThreads, 0, s>>>(A->n_groups, ns, kind, A->group_ptr, A->row_ptr, A->col_idx,
-                                                        A->vals64, dof_of, out->soff, out->tcol, out->v64, out->vhi,
+                                                        A->vals64, dof_of, out->soff, out->tcol, out->tcol16, X.wide,
+                                                        out->v64, out->vhi,
                                                         out->vlo, out->gmask, out->S, X.err);
   count_launches(1);
   FEAB_CHECK_LAUNCH();
-  int32_t err = 0;
-  FEAB_CUDA(cudaMemcpyAsync(&err, X.err, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+  int32_t flags[2] = {0, 0};
+  FEAB_CUDA(cudaMemcpyAsync(flags, X.err, 2 * sizeof(int32_t), cudaMemcpyDeviceToHost, s));
   FEAB_CUDA(cudaStreamSynchronize(s));
-  return err ? FEAB_BAD_ARG : FEAB_OK;
+  if (flags[1]) out->tcol16 = nullptr;  // some offset needs more than 16 bits: the SpMV reads tcol
+  return flags[0] ? FEAB_BAD_ARG : FEAB_OK;
 }
 
 
@@ -269,7 +285,7 @@ extern "C" int32_t feab_sell_spmv(const feab_csr* A, const feab_sell_operator* o
     return FEAB_BAD_ARG;
   if (op->kind != FEAB_PREC_FP64 && op->kind != FEAB_PREC_MIXED) return FEAB_BAD_ARG;
   auto al = [](const void* p, uintptr_t a) { return (reinterpret_cast<uintptr_t>(p) & (a - 1)) == 0; };
-  if (!op->soff || !op->tcol || !al(op->tcol, 16)) return FEAB_BAD_ARG;
+  if (!op->soff || !op->tcol || !al(op->tcol, 16) || (op->tcol16 && !al(op->tcol16, 8))) return FEAB_BAD_ARG;
   if (op->kind == FEAB_PREC_FP64 ? (!op->v64 || !al(op->v64, 16))
                                  : (!op->vhi || !op->vlo || !op->gmask || !op->S || !al(op->vhi, 16) || !al(op->vlo, 8)))
     return FEAB_BAD_ARG;

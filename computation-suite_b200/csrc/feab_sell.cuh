@@ -7,6 +7,8 @@
 // (b = soff[s] + 4i) and lane l:
 //   columns    tcol[b * 32 + 4 l + u]                 u = 0..3, the 4 steps of the block
 //   row k      value[(3 b + 4 k) * 32 + 4 l + u]      k = 0..2
+// (or, when every column lies within 16 bits of the lane's first row, the 2-byte offsets
+//   tcol16[b * 32 + 4 l + u] = column - r0, one 8-byte load per block),
 // so per block a lane issues one 16-byte column load and, per row, one 16-byte (32-bit hi words)
 // + one 8-byte (16-bit lo words) load, or two 16-byte FP64 loads; the warp's loads are 512 (or
 // 256) contiguous bytes.  A lane accumulates its rows alone, in column order, with no cross-lane
@@ -67,6 +69,7 @@ struct SellView {
   int n_slices, n_groups;
   const int32_t* soff;
   const int32_t* tcol;
+  const int16_t* tcol16;    // 2-byte column offsets from the lane's first row (or NULL)
   const double* v64;
   const uint32_t* vhi;
   const uint16_t* vlo;
@@ -106,7 +109,7 @@ struct SellTuning {
 // difference form sum_{b != a} w (x_b - x_a) + S x_a, evaluated as sum_{b != a} w x_b + T x_a
 // with T = S - sum_{b != a} w precomputed (the same value exactly, so the same rounding error of
 // the 36-bit values); xs[j] = x of the node's own DOF component j (0 when that component is fixed).
-template <int KIND, typename XF>
+template <int KIND, bool IDX16, typename XF>
 __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lane, const SellLane& L, XF xf,
                                            double (&acc)[3], double (&xs)[3]) {
   constexpr int NB = SellTuning<KIND>::kBlocks;
@@ -144,11 +147,19 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
     for (int nb = 0; nb < NB; ++nb) {
       if (nb > 0 && j + 4 * nb >= W) break;
       const size_t b = (size_t)(base + j + 4 * nb);
-      const uint4 tq = ld_op(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
-      t[nb][0] = tq.x;
-      t[nb][1] = tq.y;
-      t[nb][2] = tq.z;
-      t[nb][3] = tq.w;
+      if (IDX16) {
+        const uint2 tq = ld_op(reinterpret_cast<const uint2*>(V.tcol16 + b * 32) + lane);
+        t[nb][0] = (unsigned)(L.r0 + (int)(int16_t)(tq.x & 0xffffu));
+        t[nb][1] = (unsigned)(L.r0 + (int)(int16_t)(tq.x >> 16));
+        t[nb][2] = (unsigned)(L.r0 + (int)(int16_t)(tq.y & 0xffffu));
+        t[nb][3] = (unsigned)(L.r0 + (int)(int16_t)(tq.y >> 16));
+      } else {
+        const uint4 tq = ld_op(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
+        t[nb][0] = tq.x;
+        t[nb][1] = tq.y;
+        t[nb][2] = tq.z;
+        t[nb][3] = tq.w;
+      }
       if (KIND == FEAB_PREC_FP64) {
 #pragma unroll
         for (int k = 0; k < 3; ++k) {

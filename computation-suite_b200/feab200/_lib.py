@@ -48,7 +48,7 @@ class DiffOperator(C.Structure):
 class SellOperator(C.Structure):
     _fields_ = [("kind", C.c_int32), ("n_slices", C.c_int32), ("soff", C.c_void_p), ("tcol", C.c_void_p),
                 ("v64", C.c_void_p), ("vhi", C.c_void_p), ("vlo", C.c_void_p), ("gmask", C.c_void_p),
-                ("S", C.c_void_p)]
+                ("S", C.c_void_p), ("tcol16", C.c_void_p)]
 
 
 class Batch(C.Structure):

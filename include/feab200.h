@@ -115,6 +115,9 @@ typedef struct feab_sell_operator {
   uint16_t* vlo;     /* MIXED kind: 96 per step                                 */
   uint8_t* gmask;    /* MIXED kind: n_groups free-DOF masks                     */
   double* S;         /* MIXED kind: 3 n own-node terms T = S - W               */
+  int16_t* tcol16;   /* 32 per step: column - the lane's first row, when every  */
+                     /* such offset fits 16 bits (NULL otherwise); the SpMV    */
+                     /* then reads these 2-byte offsets instead of tcol        */
 } feab_sell_operator;
 
 typedef struct feab_pcg_params {

@@ -86,3 +86,33 @@ def test_pcg_through_both_layouts_matches_direct_solve(golden):
         assert abs(info.iters - int(g["pcg_iters"])) <= 2, (precision, layout, info.iters)
         err = np.linalg.norm(x.cpu().numpy() - u_ref) / np.linalg.norm(u_ref)
         assert err < 1e-8, (precision, layout, err)
+
+
+def test_sell_column_offsets_16_bit_and_wide():
+    """The sliced operator stores 2-byte column offsets from each lane's first row when they all
+    fit 16 bits, and keeps the 4-byte columns otherwise (a 110 x 100 x 1 box: the second node
+    layer lies 11,211 nodes, 33,633 DOFs, above the first).  Both forms give the CSR product,
+    and the PCG through either converges to the same solution."""
+    from feab200.device import pcg_solve
+    rng = np.random.default_rng(17)
+    cases = {}
+    for shape in ((12, 4, 3), (110, 100, 1)):
+        nodes, el = O.box_mesh(2.0, 1.0, 0.1, *shape)
+        D = O.D_solid3d(5.0, 0.3)
+        fixed = O.fixed_dofs_on_plane(nodes, 0, 0.0)
+        n_dof = 3 * len(nodes)
+        op = _reduced(nodes, el, D, fixed)
+        free = O.free_dofs(n_dof, fixed)
+        Kff = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(nodes[el], D), el, n_dof), free)
+        _check(op, Kff, (rng.standard_normal(op.n),))
+        cases[shape] = (op, Kff)
+    assert cases[(12, 4, 3)][0].sell_operator("fp64").tcol16
+    assert cases[(12, 4, 3)][0].sell_operator("mixed").tcol16
+    assert not cases[(110, 100, 1)][0].sell_operator("fp64").tcol16
+    assert not cases[(110, 100, 1)][0].sell_operator("mixed").tcol16
+    op, Kff = cases[(110, 100, 1)]
+    b = rng.standard_normal(op.n)
+    x64, i64 = pcg_solve(op, b, tol=1e-10, precision="fp64", layout="sell")
+    xcs, ics = pcg_solve(op, b, tol=1e-10, precision="fp64", layout="csr")
+    assert i64.status == 0 and ics.status == 0
+    assert float(torch.linalg.norm(x64 - xcs) / torch.linalg.norm(xcs)) < 1e-8

@@ -582,7 +582,7 @@ def workload_batch(args):
             "total_dof_rank0": n_dof, "total_rhs_rank0": n_rhs,
             "iters": {"max": int(r.iters.max()), "mean_active": float(r.iters[r.iters > 0].mean())},
             "rel_err_max_vs_fp64_tight": float(max(errs)), "status_ok": bool((r.status == 0).all()),
-            "launch_shape": {k: {"item_groups": v.item_groups, "tile_width": v.tile_width,
+            "launch_shape": {k: {"item_groups": v.item_groups, "tile_width": v.tile_width, "node_tiles": v.node_tiles,
                                  "us_per_step": round(v.us_per_step, 1)} for k, v in shapes.items()}}
 
 
@@ -640,7 +640,7 @@ def workload_snapshot(args):
     return {"metric": f"snapshot block-PCG (64 RHS) + Gram POD time, {shp} hex8",
             "value": round(res["mixed"][0] + gram8_ms + eig_ms, 2), "unit": "ms",
             "block_pcg_ms": {"mixed": round(res["mixed"][0], 2), "fp64": round(res["fp64"][0], 2)},
-            "launch_shape": {k: {"item_groups": v.item_groups, "tile_width": v.tile_width,
+            "launch_shape": {k: {"item_groups": v.item_groups, "tile_width": v.tile_width, "node_tiles": v.node_tiles,
                                  "us_per_step": round(v.us_per_step, 1)} for k, v in tuned.items()},
             "gram_ms": round(gram_ms, 4), "eig_ms": round(eig_ms, 3),
             "gram_roofline": {"bound": "hbm", "achieved": round(gram_bytes / (gram_ms * 1e-3) / 1e9, 1), "peak": peak,
@@ -1005,7 +1005,7 @@ def workload_block_step(args):
             a, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record()
             block_pcg(op, b.row_bounds, B, [k], tol=0.0, maxiter=m, precision=prec, max_groups=shape.item_groups,
-                      tile_width=shape.tile_width, tune=False)
+                      tile_width=shape.tile_width, tune=False, node_tiles=shape.node_tiles)
             e.record()
             e.synchronize()
             return a.elapsed_time(e)
@@ -1013,7 +1013,7 @@ def workload_block_step(args):
             run(4)
         t4, tl = min(run(4) for _ in range(2)), min(run(long) for _ in range(2))
         out[prec] = {"us_per_step": round((tl - t4) * 1e3 / (long - 4), 1), "item_groups": shape.item_groups,
-                     "tile_width": shape.tile_width}
+                     "tile_width": shape.tile_width, "node_tiles": shape.node_tiles}
     flush = L2Flush(op.vals64.device)
     Y = torch.empty_like(B)
     block_spmm(op, B, out=Y)

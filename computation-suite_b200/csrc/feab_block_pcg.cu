@@ -78,6 +78,19 @@ struct BArgs {
   int32_t* remaining;
   double tol, delta;
   int32_t maxiter;
+  // node tiles (feab_tile_operator; t_g0 == null: the SpMM walks single row groups)
+  const int32_t* t_g0;
+  const int32_t* t_gt;
+  const int32_t* t_uoff;
+  const int32_t* t_poff;
+  const int32_t* t_ucol;
+  const uint8_t* t_umask;
+  const double* t_v64;
+  const uint32_t* t_vhi;
+  const uint16_t* t_vlo;
+  const uint8_t* t_vlo2;
+  const int32_t* t_cptr;
+  const int32_t* t_chunk;
 };
 
 // True in the block that completes the last of problem p's n_items_p work items; `count` items
@@ -344,171 +357,237 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
   }
 }
 
-// ---------------------------------------------------------------- pipelined group staging
-// 1: in the SpMM of step A (panels of 32 or 64 columns), a warp copies the next row group's
-// columns and values into shared memory with cp.async while it gathers and multiplies the current
-// one (two raw stages per warp, dynamic shared memory), so the staging latency is off the
-// critical path.  The difference form's 56-bit values are copied as stored and decoded when read.
-#ifndef FEAB_BLOCK_PIPE
-#define FEAB_BLOCK_PIPE 0
+// ---------------------------------------------------------------- node tiles
+// A warp applies a tile of up to kTG consecutive row groups (feab_tile_operator): it walks the
+// union of their column lists, gathers each union column's panel row once and adds it, with the
+// column's value triple of each group that has the column, to that group's rows.  The union is
+// staged in chunks of kTileChunk columns: the columns, the group masks, each column's first
+// value triple within the chunk (a warp scan of the mask popcounts) and the chunk's values
+// (decoded to FP64 for the difference form).  The tile's columns are grouped by mask, so a chunk
+// is a few runs of one mask each, and each run goes through a loop specialised for its mask.
+constexpr int kTG = FEAB_TILE_GROUPS;
+constexpr int kTileChunk = FEAB_TILE_CHUNK;
+// union columns whose panel rows a lane gathers before using any
+#ifndef FEAB_TILE_UNROLL
+#define FEAB_TILE_UNROLL 8
 #endif
+constexpr int kTileU = FEAB_TILE_UNROLL;
 
-struct __align__(16) RawStage {  // the same size as GroupStage, which it stands in for
-  int col[kStageCols];
-  union {
-    double v64[3][kStageCols];
-    struct {
-      uint32_t hi[3][kStageCols];
-      uint16_t lo[3][kStageCols];
-      uint8_t lo2[3][kStageCols];
-    } d;
-  };
-};
-static_assert(sizeof(RawStage) == sizeof(GroupStage), "a raw stage doubles as a synchronous stage");
-
-__device__ __forceinline__ uint32_t shared_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
-}
 __device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(shared_u32(dst)), "l"(src) : "memory");
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
 }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
 
-// Start the copies of group g's columns and values into st; false (nothing issued) when the
-// group does not fit one stage.  Rows the group does not have are zero-filled.
-template <bool DIFF>
-__device__ __forceinline__ bool stage_issue(const BArgs& A, int g, int lane, RawStage& st) {
-  const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
-  if (DIFF) {
-    const int c0 = A.goff[g], s0 = A.voff[g], len = A.goff[g + 1] - c0;
-    if (len > kStageCols) return false;
-    for (int mq = lane; mq < (len >> 2); mq += 32) {
-      const int m = 4 * mq;
-      cp_async16(&st.col[m], A.tcol + c0 + m);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        if (k < f) {
-          cp_async16(&st.d.hi[k][m], A.vhi + s0 + k * len + m);
-          cp_async8(&st.d.lo[k][m], A.vlo + s0 + k * len + m);
-          cp_async4(&st.d.lo2[k][m], A.vlo2 + s0 + k * len + m);
-        } else {
-          *reinterpret_cast<uint4*>(&st.d.hi[k][m]) = make_uint4(0u, 0u, 0u, 0u);
-          *reinterpret_cast<uint2*>(&st.d.lo[k][m]) = make_uint2(0u, 0u);
-          *reinterpret_cast<uint32_t*>(&st.d.lo2[k][m]) = 0u;
-        }
-      }
-    }
-  } else {
-    const int s0 = A.row_ptr[r0], len = A.row_ptr[r0 + 1] - s0;
-    if (len > kStageCols) return false;
-    for (int m = lane; m < len; m += 32) {
-      cp_async4(&st.col[m], A.col_idx + s0 + m);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        if (k < f) cp_async8(&st.v64[k][m], A.vals64 + s0 + k * len + m);
-        else st.v64[k][m] = 0.0;
-      }
-    }
-  }
-  cp_async_commit();
-  return true;
-}
+struct __align__(16) TileStage {
+  int col[kTileChunk];
+  uint16_t pair[kTileChunk];
+  uint32_t mask4[kTileChunk / 4];
+  double val[3 * kTG * kTileChunk];
+};
 
-// The SpMM of group g from a stage filled by stage_issue (one sub-warp, K >= 32).
-template <int K, bool DIFF>
-__device__ __forceinline__ void group_spmm_staged(const BArgs& A, int g, int lane, const RawStage& st,
-                                                  const double* __restrict__ src, double (&acc)[3][K / 32]) {
-  constexpr int CPL = K / 32;
-  const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
-  const int nc = DIFF ? A.goff[g + 1] - A.goff[g] : A.row_ptr[r0 + 1] - A.row_ptr[r0];
+// A warp's shared-memory stage: one row group's columns and values, or one tile chunk.
+union __align__(16) WarpStage {
+  GroupStage g;
+  TileStage t;
+};
+
+constexpr int popc4(int m) { return (m & 1) + ((m >> 1) & 1) + ((m >> 2) & 1) + ((m >> 3) & 1); }
+static_assert(kTG >= 1 && kTG <= 4, "tiles of 1 to 4 row groups (4-bit group masks)");
+
+// Staged columns [mb, me) of one mask M: each column's value triples (one per set bit of M, in
+// bit order) are contiguous from value vb, so the loop is free of per-group branches.
+template <int M, int K>
+__device__ __forceinline__ void tile_run(const int* __restrict__ col, const double* __restrict__ val, int mb, int me,
+                                         int vb, int sub, int cl, const double* __restrict__ src,
+                                         double (&acc)[kTG][3][K >= 32 ? K / 32 : 1]) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int MPW = K >= 32 ? 1 : 32 / K;
+  constexpr int U = kTileU;
+  constexpr int NB = popc4(M);
+  for (int m0 = mb + sub; m0 < me; m0 += MPW * U) {
+    double xv[U][CPL];
 #pragma unroll
-  for (int k = 0; k < 3; ++k)
-#pragma unroll
-    for (int q = 0; q < CPL; ++q) acc[k][q] = 0.0;
-  double xs[3][CPL];
-  if (DIFF) {
-    const int mask = A.gmask[g];
-#pragma unroll
-    for (int j = 0; j < 3; ++j) {
-      if ((mask >> j) & 1) {
-        gather_row<K>(src, r0 + __popc(mask & ((1 << j) - 1)), lane, xs[j]);
-      } else {
-#pragma unroll
-        for (int q = 0; q < CPL; ++q) xs[j][q] = 0.0;
-      }
-    }
-  }
-  for (int m0 = 0; m0 < nc; m0 += kUnroll) {
-    unsigned t[kUnroll];
-    double xv[kUnroll][CPL];
-#pragma unroll
-    for (int u4 = 0; u4 < kUnroll / 4; ++u4) {
-      const int4 tq = *reinterpret_cast<const int4*>(&st.col[m0 + 4 * u4]);
-      t[4 * u4] = (unsigned)tq.x;
-      t[4 * u4 + 1] = (unsigned)tq.y;
-      t[4 * u4 + 2] = (unsigned)tq.z;
-      t[4 * u4 + 3] = (unsigned)tq.w;
-    }
-#pragma unroll
-    for (int u = 0; u < kUnroll; ++u) {
-      if (m0 + u < nc) {
-        gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), lane, xv[u]);
+    for (int u = 0; u < U; ++u) {
+      const int m = m0 + u * MPW;
+      if (m < me) {
+        gather_row<K>(src, col[m], cl, xv[u]);
       } else {
 #pragma unroll
         for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;
       }
     }
 #pragma unroll
-    for (int u2 = 0; u2 < kUnroll / 2; ++u2) {
-      const int m = m0 + 2 * u2;
-      if (m >= nc) break;
-      double2 w[3];
+    for (int u = 0; u < U; ++u) {
+      const int m = m0 + u * MPW;
+      if (m >= me) break;
+      const double* w = &val[vb + 3 * NB * (m - mb)];
+      int b = 0;
+#pragma unroll
+      for (int j = 0; j < kTG; ++j) {
+        if ((M >> j) & 1) {
+          const double w0 = w[3 * b], w1 = w[3 * b + 1], w2 = w[3 * b + 2];
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) {
+            acc[j][0][q] = fma(w0, xv[u][q], acc[j][0][q]);
+            acc[j][1][q] = fma(w1, xv[u][q], acc[j][1][q]);
+            acc[j][2][q] = fma(w2, xv[u][q], acc[j][2][q]);
+          }
+          ++b;
+        }
+      }
+    }
+  }
+}
+
+// tile_run for the run's mask mk (1 .. 2^kTG - 1): a chain of uniform branches.
+template <int M, int K>
+__device__ __forceinline__ void dispatch_run(unsigned mk, const int* __restrict__ col, const double* __restrict__ val,
+                                             int mb, int me, int vb, int sub, int cl, const double* __restrict__ src,
+                                             double (&acc)[kTG][3][K >= 32 ? K / 32 : 1]) {
+  if (mk == (unsigned)M) {
+    tile_run<M, K>(col, val, mb, me, vb, sub, cl, src, acc);
+  } else if constexpr (M + 1 < (1 << kTG)) {
+    dispatch_run<M + 1, K>(mk, col, val, mb, me, vb, sub, cl, src, acc);
+  }
+}
+
+// acc[j][row][q] = (K src) for row `row` of group j of tile t, panel column panel_col(cl, q).
+// Each chunk is staged in one round trip (columns and masks through registers, FP64 values by
+// cp.async straight to shared memory); the next chunk's descriptor is loaded meanwhile.  (A
+// variant that copied the next chunk in while applying this one, two buffers per warp, measured
+// 507 against 436 us per 128x32x32 SpMM with 64 columns: the gathers set the pace, and its larger
+// code missed in the instruction cache.)
+template <int K, bool DIFF>
+__device__ __forceinline__ void tile_spmm(const BArgs& A, int t, int lane, TileStage& st,
+                                          const double* __restrict__ src,
+                                          double (&acc)[kTG][3][K >= 32 ? K / 32 : 1]) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int LW = K >= 32 ? 32 : K;
+  const int sub = lane / LW, cl = lane % LW;
+  const int4* __restrict__ chunks = reinterpret_cast<const int4*>(A.t_chunk);
+  const int c1 = A.t_cptr[t + 1];
+  int c = A.t_cptr[t];
+#pragma unroll
+  for (int j = 0; j < kTG; ++j)
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) acc[j][k][q] = 0.0;
+  // chunk descriptor {first union column, columns, first value, values}
+  int4 d = c < c1 ? __ldg(chunks + c) : make_int4(0, 0, 0, 0);
+  for (; c < c1; ++c) {
+    const int4 dn = c + 1 < c1 ? __ldg(chunks + c + 1) : d;
+    const int nc = d.y, nv = d.w;  // nc a multiple of 4
+    if (!DIFF) {
+      for (int i = lane; i < nv; i += 32) cp_async8(&st.val[i], A.t_v64 + (int64_t)d.z + i);
+      cp_async_commit();
+    } else {
+      for (int i = lane; i < nv; i += 32) {
+        const int64_t q = (int64_t)d.z + i;
+        st.val[i] = dec56(__ldg(A.t_vhi + q), __ldg(A.t_vlo + q), __ldg(A.t_vlo2 + q));
+      }
+    }
+    int np = 0, p4[4] = {0, 0, 0, 0};
+    if (4 * lane < nc) {
+      const int4 c4 = __ldg(reinterpret_cast<const int4*>(A.t_ucol + d.x) + lane);
+      const uint32_t m4 = __ldg(reinterpret_cast<const uint32_t*>(A.t_umask + d.x) + lane);
+      *reinterpret_cast<int4*>(&st.col[4 * lane]) = c4;
+      st.mask4[lane] = m4;
+#pragma unroll
+      for (int e = 0; e < 4; ++e) p4[e] = __popc((m4 >> (8 * e)) & 0xffu);
+      np = p4[0] + p4[1] + p4[2] + p4[3];
+    }
+    // the first value triple of every column within the chunk: a warp scan of mask popcounts
+    const int incl = warp_incl_scan(np, lane);
+    if (4 * lane < nc) {
+      int e = incl - np;
+#pragma unroll
+      for (int q = 0; q < 4; ++q) {
+        st.pair[4 * lane + q] = (uint16_t)e;
+        e += p4[q];
+      }
+    }
+    if (!DIFF) cp_async_wait_all();
+    __syncwarp();
+    // runs of columns with the same mask (a tile's columns are grouped by mask; padding, mask
+    // 0, comes last)
+    int m = 0;
+    while (m < nc) {
+      const unsigned mk = (st.mask4[m >> 2] >> (8 * (m & 3))) & 0xffu;
+      if (mk == 0u) break;
+      int e = m;
+      while (true) {
+        const int q = e + lane;
+        const bool other = q >= nc || ((st.mask4[q >> 2] >> (8 * (q & 3))) & 0xffu) != mk;
+        const unsigned bal = __ballot_sync(FEAB_FULL_MASK, other);
+        if (bal) {
+          e += __ffs(bal) - 1;
+          break;
+        }
+        e += 32;
+      }
+      dispatch_run<1, K>(mk, st.col, st.val, m, e, 3 * st.pair[m], sub, cl, src, acc);
+      m = e;
+    }
+    __syncwarp();  // every lane is done with the stage before it is refilled
+    d = dn;
+  }
+  // combine the sub-warps (lanes with equal cl)
+#pragma unroll
+  for (int o = LW; o < 32; o <<= 1)
+#pragma unroll
+    for (int j = 0; j < kTG; ++j)
+#pragma unroll
+      for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int q = 0; q < CPL; ++q) acc[j][k][q] += __shfl_xor_sync(FEAB_FULL_MASK, acc[j][k][q], o);
+  if constexpr (DIFF) {
+    // the own-node term T_a x_a of every group (the difference form leaves own columns out)
+    const int g0 = A.t_g0[t], nt = A.t_g0[t + 1] - g0;
+#pragma unroll
+    for (int j = 0; j < kTG; ++j) {
+      if (j >= nt) break;
+      const int g = g0 + j;
+      const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+      const int mask = A.gmask[g];
+      double xs[3][CPL];
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) {
+        if ((mask >> cc) & 1) {
+          gather_row<K>(src, r0 + __popc(mask & ((1 << cc) - 1)), cl, xs[cc]);
+        } else {
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) xs[cc][q] = 0.0;
+        }
+      }
 #pragma unroll
       for (int k = 0; k < 3; ++k) {
-        if (DIFF) {
-          const uint2 h = *reinterpret_cast<const uint2*>(&st.d.hi[k][m]);
-          const uint32_t l = *reinterpret_cast<const uint32_t*>(&st.d.lo[k][m]);
-          const uint32_t l2 = *reinterpret_cast<const uint16_t*>(&st.d.lo2[k][m]);
-          w[k] = make_double2(dec56(h.x, l, l2), dec56(h.y, l >> 16, l2 >> 8));
-        } else {
-          w[k] = *reinterpret_cast<const double2*>(&st.v64[k][m]);
-        }
-      }
-      const bool two = m + 1 < nc;  // a column past nc has xv = 0 but a stale value
+        if (k < f) {
+          const double s0v = A.S[(int64_t)(r0 + k) * 3 + 0], s1v = A.S[(int64_t)(r0 + k) * 3 + 1],
+                       s2v = A.S[(int64_t)(r0 + k) * 3 + 2];
 #pragma unroll
-      for (int q = 0; q < CPL; ++q) {
-        const double d = xv[2 * u2][q];
-        acc[0][q] = fma(w[0].x, d, acc[0][q]);
-        acc[1][q] = fma(w[1].x, d, acc[1][q]);
-        acc[2][q] = fma(w[2].x, d, acc[2][q]);
-      }
-      if (two) {
-#pragma unroll
-        for (int q = 0; q < CPL; ++q) {
-          const double d = xv[2 * u2 + 1][q];
-          acc[0][q] = fma(w[0].y, d, acc[0][q]);
-          acc[1][q] = fma(w[1].y, d, acc[1][q]);
-          acc[2][q] = fma(w[2].y, d, acc[2][q]);
+          for (int q = 0; q < CPL; ++q) acc[j][k][q] += s0v * xs[0][q] + s1v * xs[1][q] + s2v * xs[2][q];
         }
       }
     }
   }
-  if (DIFF) {
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      if (k < f) {
-        const double s0v = A.S[(int64_t)(r0 + k) * 3 + 0], s1v = A.S[(int64_t)(r0 + k) * 3 + 1],
-                     s2v = A.S[(int64_t)(r0 + k) * 3 + 2];
-#pragma unroll
-        for (int q = 0; q < CPL; ++q) acc[k][q] += s0v * xs[0][q] + s1v * xs[1][q] + s2v * xs[2][q];
-      }
-    }
-  }
+}
+
+// The item's tiles [t0, t1): its groups are whole tiles (checked before the solve starts).
+__device__ __forceinline__ void item_tiles(const BArgs& A, int it, int& t0, int& t1) {
+  t0 = A.t_gt[A.item_g0[it]];
+  t1 = A.t_gt[A.item_g1[it] - 1] + 1;
+}
+
+// Every work item starts and ends on a tile boundary; flag[0] = 1 otherwise.
+__global__ void k_tile_items_check(BArgs A, int32_t* flag) {
+  const int it = blockIdx.x * blockDim.x + threadIdx.x;
+  if (it >= A.n_items) return;
+  const int g0 = A.item_g0[it], g1 = A.item_g1[it];
+  if (g0 < 0 || g1 <= g0 || g1 > A.n_groups || A.t_g0[A.t_gt[g0]] != g0 || A.t_g0[A.t_gt[g1 - 1] + 1] != g1)
+    atomicExch(flag, 1);
 }
 
 // setup: R = B - 0 (x0 = 0), P = M R, per column ||b||, r.z; columns beyond the problem's
@@ -586,12 +665,10 @@ template <int K, bool MIXED>
 __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
-  constexpr bool PIPE = FEAB_BLOCK_PIPE && K >= 32;
   __shared__ double sm[kWarps][K];
-  __shared__ GroupStage stage[PIPE ? 1 : kWarps];
-  extern __shared__ __align__(16) unsigned char dyn_stage[];  // PIPE: two raw stages per warp
+  extern __shared__ __align__(16) unsigned char dyn_stage[];  // one WarpStage per warp
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  RawStage* rs = reinterpret_cast<RawStage*>(dyn_stage) + 2 * w;
+  WarpStage& stage = reinterpret_cast<WarpStage*>(dyn_stage)[w];
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
     const ProbState P = A.ps[p];
@@ -603,57 +680,58 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
     double part[CPL];
 #pragma unroll
     for (int q = 0; q < CPL; ++q) part[q] = 0.0;
-    const int g1 = A.item_g1[it];
-    int buf = 0;
-    bool staged = false;
-    if constexpr (PIPE) {
-      const int g = A.item_g0[it] + w;
-      if (g < g1) staged = diff ? stage_issue<true>(A, g, lane, rs[0]) : stage_issue<false>(A, g, lane, rs[0]);
-    }
-    for (int g = A.item_g0[it] + w; g < g1; g += kWarps) {
-      double acc[3][CPL];
-      if constexpr (PIPE) {
-        // group g's copies have landed; start group g + kWarps's into the other stage
-        cp_async_wait_all();
-        __syncwarp();
-        bool staged_next = false;
-        const int gn = g + kWarps;
-        if (gn < g1)
-          staged_next = diff ? stage_issue<true>(A, gn, lane, rs[buf ^ 1]) : stage_issue<false>(A, gn, lane, rs[buf ^ 1]);
-        if (staged) {
-          if (diff) group_spmm_staged<K, true>(A, g, lane, rs[buf], src, acc);
-          else group_spmm_staged<K, false>(A, g, lane, rs[buf], src, acc);
+    // one output row: AP and p.Ap, or (reliable step) R = B - K X and r.r
+    auto emit = [&](int row, const double (&v)[CPL]) {
+#pragma unroll
+      for (int q = 0; q < CPL; ++q) {
+        const int64_t idx = (int64_t)row * K + panel_col<K>(lane, q);
+        if (reliable) {
+          const double ri = A.B[idx] - v[q];
+          A.R[idx] = ri;
+          part[q] += ri * ri;
         } else {
-          GroupStage& gs = *reinterpret_cast<GroupStage*>(&rs[buf]);
-          if (diff) group_spmm<K, MIXED>(A, g, lane, gs, src, acc);
-          else group_spmm<K, false>(A, g, lane, gs, src, acc);
+          const double pv = po[idx];
+          A.AP[idx] = v[q];
+          part[q] += pv * v[q];
         }
-        __syncwarp();  // every lane is done with rs[buf] before it is refilled
-        staged = staged_next;
-        buf ^= 1;
-      } else if constexpr (MIXED) {
-        if (!diff) group_spmm<K, false>(A, g, lane, stage[w], src, acc);
-        else group_spmm<K, true>(A, g, lane, stage[w], po, acc);
-      } else {
-        group_spmm<K, false, kUnrollFp64>(A, g, lane, stage[w], po, acc);
       }
-      if (lane < LW) {
-        const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+    };
+    if (A.t_g0 && !reliable) {
+      int t0, t1;
+      item_tiles(A, it, t0, t1);
+      for (int t = t0 + w; t < t1; t += kWarps) {
+        double acc[kTG][3][CPL];
+        tile_spmm<K, MIXED>(A, t, lane, stage.t, po, acc);
+        if (lane < LW) {
+          const int tg0 = A.t_g0[t], nt = A.t_g0[t + 1] - tg0;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (k >= f) break;
+          for (int j = 0; j < kTG; ++j) {
+            if (j >= nt) break;
+            const int r0 = A.group_ptr[tg0 + j], f = A.group_ptr[tg0 + j + 1] - r0;
 #pragma unroll
-          for (int q = 0; q < CPL; ++q) {
-            const int64_t idx = (int64_t)(r0 + k) * K + panel_col<K>(lane, q);
-            if (reliable) {
-              const double ri = A.B[idx] - acc[k][q];
-              A.R[idx] = ri;
-              part[q] += ri * ri;
-            } else {
-              const double pv = po[idx];
-              A.AP[idx] = acc[k][q];
-              part[q] += pv * acc[k][q];
+            for (int k = 0; k < 3; ++k) {
+              if (k >= f) break;
+              emit(r0 + k, acc[j][k]);
             }
+          }
+        }
+      }
+    } else {
+      const int g1 = A.item_g1[it];
+      for (int g = A.item_g0[it] + w; g < g1; g += kWarps) {
+        double acc[3][CPL];
+        if constexpr (MIXED) {
+          if (!diff) group_spmm<K, false>(A, g, lane, stage.g, src, acc);
+          else group_spmm<K, true>(A, g, lane, stage.g, po, acc);
+        } else {
+          group_spmm<K, false, kUnrollFp64>(A, g, lane, stage.g, po, acc);
+        }
+        if (lane < LW) {
+          const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
+#pragma unroll
+          for (int k = 0; k < 3; ++k) {
+            if (k >= f) break;
+            emit(r0 + k, acc[k]);
           }
         }
       }
@@ -993,10 +1071,51 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_block_spmm(BArgs 
   }
 }
 
+// The same through the node tiles (FP64 tile values), one warp per tile.
 template <int K>
-void launch_block_spmm(const BArgs& A, const double* X, double* Y, cudaStream_t s) {
-  const int grid = std::max(1, std::min((A.n_groups + kWarps - 1) / kWarps, sm_count() * 8));
-  k_block_spmm<K><<<grid, kThreads, 0, s>>>(A, X, Y);
+__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_block_spmm_tiles(BArgs A, int32_t n_tiles,
+                                                                               const double* __restrict__ src,
+                                                                               double* __restrict__ dst) {
+  constexpr int CPL = K >= 32 ? K / 32 : 1;
+  constexpr int LW = K >= 32 ? 32 : K;
+  extern __shared__ __align__(16) unsigned char dyn_stage[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  WarpStage& stage = reinterpret_cast<WarpStage*>(dyn_stage)[w];
+  for (int t = blockIdx.x * kWarps + w; t < n_tiles; t += gridDim.x * kWarps) {
+    double acc[kTG][3][CPL];
+    tile_spmm<K, false>(A, t, lane, stage.t, src, acc);
+    if (lane < LW) {
+      const int tg0 = A.t_g0[t], nt = A.t_g0[t + 1] - tg0;
+#pragma unroll
+      for (int j = 0; j < kTG; ++j) {
+        if (j >= nt) break;
+        const int r0 = A.group_ptr[tg0 + j], f = A.group_ptr[tg0 + j + 1] - r0;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+          if (k >= f) break;
+#pragma unroll
+          for (int q = 0; q < CPL; ++q) dst[(int64_t)(r0 + k) * K + panel_col<K>(lane, q)] = acc[j][k][q];
+        }
+      }
+    }
+  }
+}
+
+constexpr size_t kStageBytes = kWarps * sizeof(WarpStage);
+
+template <int K>
+cudaError_t launch_block_spmm(const BArgs& A, int32_t n_tiles, const double* X, double* Y, cudaStream_t s) {
+  if (A.t_g0) {
+    cudaError_t e = cudaFuncSetAttribute(k_block_spmm_tiles<K>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)kStageBytes);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min((n_tiles + kWarps - 1) / kWarps, sm_count() * 8));
+    k_block_spmm_tiles<K><<<grid, kThreads, kStageBytes, s>>>(A, n_tiles, X, Y);
+  } else {
+    const int grid = std::max(1, std::min((A.n_groups + kWarps - 1) / kWarps, sm_count() * 8));
+    k_block_spmm<K><<<grid, kThreads, 0, s>>>(A, X, Y);
+  }
+  return cudaGetLastError();
 }
 
 size_t a256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -1021,7 +1140,7 @@ BLayout blayout(int32_t n, int32_t k, int32_t n_problems, int32_t n_items) {
   L.o_part = take(sizeof(double) * 2 * (size_t)k * (size_t)n_items);
   L.o_ps = take(sizeof(ProbState) * (size_t)n_problems);
   L.o_cs = take(sizeof(ColState) * (size_t)n_problems * (size_t)k);
-  L.o_rem = take(sizeof(int32_t));
+  L.o_rem = take(2 * sizeof(int32_t));  // problems remaining, tile-alignment flag
   L.total = off;
   return L;
 }
@@ -1050,11 +1169,9 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   };
   do {
     if (fail(graphs.events(ev))) break;
-    const size_t smem_a = (FEAB_BLOCK_PIPE && K >= 32) ? 2 * kWarps * sizeof(RawStage) : 0;
-    if (smem_a) {
-      if (fail(cudaFuncSetAttribute(k_bstep_a<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
-      if (fail(cudaFuncSetAttribute(k_bstep_a<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
-    }
+    const size_t smem_a = kStageBytes;
+    if (fail(cudaFuncSetAttribute(k_bstep_a<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
+    if (fail(cudaFuncSetAttribute(k_bstep_a<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
     auto record = [&](cudaStream_t cs) {
       for (int q = 0; q < chunk; ++q) {
         if (prec == FEAB_PREC_MIXED) {
@@ -1118,6 +1235,31 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   return worst;
 }
 
+// Fills the tile fields of A from T; false if T does not fit A's groups or the precision.
+bool set_tiles(BArgs& A, const feab_tile_operator* T, int prec) {
+  if (!T) return true;
+  if (T->n_groups != A.n_groups || T->precision != prec || T->n_tiles <= 0 || !T->tile_g0 || !T->group_tile ||
+      !T->uoff || !T->poff || !T->ucol || !T->umask || !T->cptr || !T->chunk)
+    return false;
+  if ((reinterpret_cast<uintptr_t>(T->ucol) & 15) || (reinterpret_cast<uintptr_t>(T->umask) & 3) ||
+      (reinterpret_cast<uintptr_t>(T->chunk) & 15) || (T->v64 && (reinterpret_cast<uintptr_t>(T->v64) & 7)))
+    return false;
+  if (prec == FEAB_PREC_FP64 ? !T->v64 : (!T->vhi || !T->vlo || !T->vlo2)) return false;
+  A.t_g0 = T->tile_g0;
+  A.t_gt = T->group_tile;
+  A.t_uoff = T->uoff;
+  A.t_poff = T->poff;
+  A.t_ucol = T->ucol;
+  A.t_umask = T->umask;
+  A.t_v64 = T->v64;
+  A.t_vhi = T->vhi;
+  A.t_vlo = T->vlo;
+  A.t_vlo2 = T->vlo2;
+  A.t_cptr = T->cptr;
+  A.t_chunk = T->chunk;
+  return true;
+}
+
 }  // namespace
 }  // namespace feab
 
@@ -1128,10 +1270,10 @@ extern "C" size_t feab_block_pcg_workspace_bytes(int32_t n, int32_t k, int32_t n
   return blayout(n, k, n_problems, n_items).total;
 }
 
-extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_operator* D, const feab_batch* bt,
-                                        const double* dinv64, const double* B, double* X, const feab_pcg_params* prm,
-                                        void* workspace, size_t workspace_bytes, int32_t* iters_out,
-                                        double* relres_out, int32_t* status_out, cudaStream_t s) {
+extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_operator* D, const feab_tile_operator* T,
+                                        const feab_batch* bt, const double* dinv64, const double* B, double* X,
+                                        const feab_pcg_params* prm, void* workspace, size_t workspace_bytes,
+                                        int32_t* iters_out, double* relres_out, int32_t* status_out, cudaStream_t s) {
   if (!M || !bt || !dinv64 || !B || !X || !prm || !workspace || !M->group_ptr || !M->vals64) return FEAB_BAD_ARG;
   const int k = bt->k;
   if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64) return FEAB_BAD_ARG;
@@ -1191,6 +1333,17 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   A.delta = prm->reliable_delta > 0.0 && prm->reliable_delta < 1.0 ? prm->reliable_delta : 0.1;
   A.maxiter = prm->maxiter > 0 ? prm->maxiter : (int)std::min<int64_t>(10 * (int64_t)M->n, INT32_MAX / 4);
   const int chunk = prm->chunk > 0 ? std::min(prm->chunk, 256) : 16;
+  if (!set_tiles(A, T, prec)) return FEAB_BAD_ARG;
+  if (T) {  // every work item must be whole tiles
+    FEAB_CUDA(cudaMemsetAsync(A.remaining + 1, 0, sizeof(int32_t), s));
+    k_tile_items_check<<<(A.n_items + kThreads - 1) / kThreads, kThreads, 0, s>>>(A, A.remaining + 1);
+    count_launches(1);
+    FEAB_CHECK_LAUNCH();
+    int32_t bad = 0;
+    FEAB_CUDA(cudaMemcpyAsync(&bad, A.remaining + 1, sizeof(int32_t), cudaMemcpyDeviceToHost, s));
+    FEAB_CUDA(cudaStreamSynchronize(s));
+    if (bad) return FEAB_BAD_ARG;
+  }
   switch (k) {
     case 1: return run_block<1>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
     case 2: return run_block<2>(A, prec, chunk, A.maxiter, s, iters_out, relres_out, status_out);
@@ -1202,7 +1355,8 @@ extern "C" int32_t feab_block_pcg_solve(const feab_csr* M, const feab_diff_opera
   }
 }
 
-extern "C" int32_t feab_block_spmm(const feab_csr* M, const double* X, double* Y, int32_t k, cudaStream_t s) {
+extern "C" int32_t feab_block_spmm(const feab_csr* M, const feab_tile_operator* T, const double* X, double* Y,
+                                   int32_t k, cudaStream_t s) {
   if (!M || !X || !Y || M->n <= 0 || !M->row_ptr || !M->col_idx || !M->vals64 || !M->group_ptr || M->n_groups <= 0)
     return FEAB_BAD_ARG;
   if (k != 1 && k != 2 && k != 4 && k != 8 && k != 16 && k != 32 && k != 64) return FEAB_BAD_ARG;
@@ -1216,16 +1370,18 @@ extern "C" int32_t feab_block_spmm(const feab_csr* M, const double* X, double* Y
   A.col_idx = M->col_idx;
   A.group_ptr = M->group_ptr;
   A.vals64 = M->vals64;
+  if (!set_tiles(A, T, FEAB_PREC_FP64)) return FEAB_BAD_ARG;
+  const int32_t nt = T ? T->n_tiles : 0;
+  cudaError_t e;
   switch (k) {
-    case 1: launch_block_spmm<1>(A, X, Y, s); break;
-    case 2: launch_block_spmm<2>(A, X, Y, s); break;
-    case 4: launch_block_spmm<4>(A, X, Y, s); break;
-    case 8: launch_block_spmm<8>(A, X, Y, s); break;
-    case 16: launch_block_spmm<16>(A, X, Y, s); break;
-    case 32: launch_block_spmm<32>(A, X, Y, s); break;
-    default: launch_block_spmm<64>(A, X, Y, s); break;
+    case 1: e = launch_block_spmm<1>(A, nt, X, Y, s); break;
+    case 2: e = launch_block_spmm<2>(A, nt, X, Y, s); break;
+    case 4: e = launch_block_spmm<4>(A, nt, X, Y, s); break;
+    case 8: e = launch_block_spmm<8>(A, nt, X, Y, s); break;
+    case 16: e = launch_block_spmm<16>(A, nt, X, Y, s); break;
+    case 32: e = launch_block_spmm<32>(A, nt, X, Y, s); break;
+    default: e = launch_block_spmm<64>(A, nt, X, Y, s); break;
   }
   count_launches(1);
-  FEAB_CHECK_LAUNCH();
-  return FEAB_OK;
+  return e == cudaSuccess ? FEAB_OK : FEAB_CUDA_ERROR;
 }

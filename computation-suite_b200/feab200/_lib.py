@@ -51,6 +51,17 @@ class SellOperator(C.Structure):
                 ("S", C.c_void_p), ("tcol16", C.c_void_p)]
 
 
+class TileOperator(C.Structure):
+    _fields_ = [("n_tiles", C.c_int32), ("precision", C.c_int32), ("n_groups", C.c_int32), ("reserved", C.c_int32),
+                ("tile_g0", C.c_void_p), ("group_tile", C.c_void_p), ("uoff", C.c_void_p), ("poff", C.c_void_p),
+                ("ucol", C.c_void_p), ("upair", C.c_void_p), ("umask", C.c_void_p), ("v64", C.c_void_p),
+                ("vhi", C.c_void_p), ("vlo", C.c_void_p), ("vlo2", C.c_void_p), ("cptr", C.c_void_p),
+                ("chunk", C.c_void_p)]
+
+
+TILE_GROUPS = 4   # FEAB_TILE_GROUPS: node row groups per tile of the block SpMM
+
+
 class Batch(C.Structure):
     _fields_ = [("n_problems", C.c_int32), ("k", C.c_int32), ("n_items", C.c_int32), ("reserved", C.c_int32),
                 ("item_problem", C.c_void_p), ("item_group0", C.c_void_p), ("item_group1", C.c_void_p),
@@ -102,10 +113,13 @@ SIGNATURES = {
     "feab_sell_spmv": (_I32, [C.POINTER(CSR), C.POINTER(SellOperator), _P, _P, _P]),
     "feab_csr_spmv": (_I32, [C.POINTER(CSR), C.POINTER(SellOperator), _I32, _I32, _P, _P, _P]),
     "feab_block_pcg_workspace_bytes": (_SZ, [_I32, _I32, _I32, _I32]),
-    "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(Batch), _P, _P, _P,
-                                    C.POINTER(PcgParams), _P, _SZ, C.POINTER(_I32), C.POINTER(_D), C.POINTER(_I32),
-                                    _P]),
-    "feab_block_spmm": (_I32, [C.POINTER(CSR), _P, _P, _I32, _P]),
+    "feab_tile_scratch_bytes": (_SZ, [_I32, _I32]),
+    "feab_tile_operator_build": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), _P, _I32, _I32, _P, _SZ, _P, _SZ,
+                                        C.POINTER(_SZ), C.POINTER(TileOperator), _P]),
+    "feab_block_pcg_solve": (_I32, [C.POINTER(CSR), C.POINTER(DiffOperator), C.POINTER(TileOperator),
+                                    C.POINTER(Batch), _P, _P, _P, C.POINTER(PcgParams), _P, _SZ, C.POINTER(_I32),
+                                    C.POINTER(_D), C.POINTER(_I32), _P]),
+    "feab_block_spmm": (_I32, [C.POINTER(CSR), C.POINTER(TileOperator), _P, _P, _I32, _P]),
     "feab_panel_gram_workspace_bytes": (_SZ, [_I64]),
     "feab_panel_gram": (_I32, [_P, _I32, _P, _I32, _I64, _I32, _P, _P, _SZ, _P]),
     "feab_panel_small": (_I32, [_P, _I32, _I64, _I32, _P, _I32, _P, _I32, _P]),

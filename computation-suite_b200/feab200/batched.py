@@ -42,10 +42,15 @@ class BatchResult:
     relres: np.ndarray        # (P, K) final FP64 relative residual per column
 
 
+def _problem_groups(group_ptr_host, row_bounds):
+    """The first node row group of each problem, then the group count."""
+    return np.searchsorted(np.asarray(group_ptr_host, dtype=np.int64), row_bounds, side="left").astype(np.int32)
+
+
 def _work_items(group_ptr_host, row_bounds, max_groups=64):
-    """Cut each problem's node row groups into items of <= max_groups groups."""
-    gp = np.asarray(group_ptr_host, dtype=np.int64)
-    g_bounds = np.searchsorted(gp, row_bounds, side="left")
+    """Cut each problem's node row groups into items of <= max_groups groups (whole node tiles of
+    the SpMM when max_groups is a multiple of TILE_GROUPS)."""
+    g_bounds = _problem_groups(group_ptr_host, row_bounds)
     item_problem, g0s, g1s, prob_items = [], [], [], [0]
     for p in range(len(row_bounds) - 1):
         a, b = int(g_bounds[p]), int(g_bounds[p + 1])
@@ -83,9 +88,13 @@ def problem_cost(n_nodes, n_rhs):
     return 3.0 * n_nodes * panel_width(n_rhs)
 
 
+TILE_GROUPS = L.TILE_GROUPS
+
+
 def _block_pcg_call(op, item_problem, g0, g1, prob_items, B_panel, cols, tol, maxiter, precision, reliable_delta,
-                    chunk):
-    """One feab_block_pcg_solve over a panel of width B_panel.shape[1] (a power of two)."""
+                    chunk, problem_groups=None):
+    """One feab_block_pcg_solve over a panel of width B_panel.shape[1] (a power of two).  With
+    problem_groups (and items of whole tiles) the SpMM walks the operator's node tiles."""
     dev = op.vals64.device
     n, K = B_panel.shape
     P = len(prob_items) - 1
@@ -99,12 +108,13 @@ def _block_pcg_call(op, item_problem, g0, g1, prob_items, B_panel, cols, tol, ma
     B_panel = B_panel.to(dev, torch.float64).contiguous()
     prec = L.PREC_MIXED if precision == "mixed" else L.PREC_FP64
     diff = C.byref(op.diff_operator()) if precision == "mixed" else None
+    tiles = C.byref(op.tile_operator(precision, problem_groups)) if problem_groups is not None else None
     params = L.PcgParams(float(tol), int(maxiter or 0), prec, float(reliable_delta), int(chunk), 1, 0, 0)
     iters = np.zeros(P * K, np.int32)
     relres = np.zeros(P * K, np.float64)
     status = np.zeros(P, np.int32)
     csr = op.csr_struct()
-    rc = L.lib.feab_block_pcg_solve(C.byref(csr), diff, C.byref(batch), L.dptr(op.dinv64), L.dptr(B_panel),
+    rc = L.lib.feab_block_pcg_solve(C.byref(csr), diff, tiles, C.byref(batch), L.dptr(op.dinv64), L.dptr(B_panel),
                                     L.dptr(X), C.byref(params), L.dptr(ws), wbytes,
                                     iters.ctypes.data_as(C.POINTER(C.c_int32)),
                                     relres.ctypes.data_as(C.POINTER(C.c_double)),
@@ -115,14 +125,17 @@ def _block_pcg_call(op, item_problem, g0, g1, prob_items, B_panel, cols, tol, ma
 
 
 def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=None, precision="fp64",
-              reliable_delta=0.1, chunk=16, max_groups=None, tile_width=None, tune=True):
+              reliable_delta=0.1, chunk=16, max_groups=None, tile_width=None, tune=True, node_tiles=None):
     """Solve the panel B_panel (n x K, row-major, device) for the problems whose free rows are
     [row_bounds[p], row_bounds[p+1]).  Returns (X_panel, BatchResult).
 
     Launch shape: work items of ``max_groups`` node row groups, and the panel processed in
     column tiles of ``tile_width`` (each tile is its own block solve; K is streamed once per
-    tile and step).  Left as None they come from ``tuned_block_shape`` (timed once per
-    operator shape and cached) when ``tune`` is true, else 64 groups and the full width."""
+    tile and step), and ``node_tiles``: the SpMM walks tiles of TILE_GROUPS row groups with merged
+    column lists (``ReducedOperator.tile_operator``; needs max_groups a multiple of TILE_GROUPS)
+    instead of single row groups.  Left as None they come from ``tuned_block_shape`` (timed once
+    per operator shape and cached) when ``tune`` is true, else 64 groups, the full width and node
+    tiles (node tiles whenever max_groups allows them, if the shape is given)."""
     if precision not in ("fp64", "mixed"):
         raise ValueError("block PCG precision must be 'fp64' or 'mixed'")
     n, K = B_panel.shape
@@ -133,17 +146,23 @@ def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=
         if tune:
             shape = tuned_block_shape(op, row_bounds, B_panel, cols, precision)
         else:
-            shape = BlockShape(64, K, None)
+            shape = BlockShape(64, K, None, True)
         max_groups = shape.item_groups if max_groups is None else max_groups
         tile_width = shape.tile_width if tile_width is None else tile_width
+        node_tiles = shape.node_tiles if node_tiles is None else node_tiles
+    if node_tiles is None:
+        node_tiles = max_groups % TILE_GROUPS == 0
     if tile_width not in PANELS or tile_width > K:
         raise ValueError(f"tile_width must be a panel width <= {K}, got {tile_width}")
     if int(max_groups) < 1:
         raise ValueError("max_groups must be >= 1")
     gp = op.pattern.group_ptr.cpu().numpy()
     items = _work_items(gp, np.asarray(row_bounds), int(max_groups))
+    if node_tiles and max_groups % TILE_GROUPS:
+        raise ValueError(f"node tiles need work items of a multiple of {TILE_GROUPS} row groups, got {max_groups}")
+    pgroups = _problem_groups(gp, np.asarray(row_bounds)) if node_tiles else None
     if tile_width == K:
-        return _block_pcg_call(op, *items, B_panel, cols, tol, maxiter, precision, reliable_delta, chunk)
+        return _block_pcg_call(op, *items, B_panel, cols, tol, maxiter, precision, reliable_delta, chunk, pgroups)
     P = len(row_bounds) - 1
     X = torch.zeros((n, K), dtype=torch.float64, device=op.vals64.device)
     status = np.zeros(P, np.int32)
@@ -154,7 +173,7 @@ def block_pcg(op: ReducedOperator, row_bounds, B_panel, cols, tol=1e-8, maxiter=
         if not ct.any():
             continue
         Xt, rt = _block_pcg_call(op, *items, B_panel[:, c0:c0 + tile_width], ct, tol, maxiter, precision,
-                                 reliable_delta, chunk)
+                                 reliable_delta, chunk, pgroups)
         X[:, c0:c0 + tile_width] = Xt
         iters[:, c0:c0 + tile_width] = rt.iters
         relres[:, c0:c0 + tile_width] = rt.relres
@@ -171,6 +190,7 @@ class BlockShape:
     item_groups: int          # node row groups per work item (the "elements per block" of the SpMM)
     tile_width: int           # right-hand-side columns per block solve
     us_per_step: float | None  # measured cost of one block-PCG step of the whole panel
+    node_tiles: bool = False   # the SpMM walks node tiles (ReducedOperator.tile_operator)
 
 
 _tuned_block = {}
@@ -184,7 +204,7 @@ def tuning_cache_path():
 
 
 def tuning_key(device_name, n, nnz, n_problems, k, precision):
-    return f"{device_name}|n={n}|nnz={nnz}|problems={n_problems}|k={k}|{precision}"
+    return f"{device_name}|n={n}|nnz={nnz}|problems={n_problems}|k={k}|{precision}|spmm=tiles{TILE_GROUPS}"
 
 
 def load_tuning(path=None):
@@ -198,10 +218,12 @@ def load_tuning(path=None):
     for key, v in raw.items() if isinstance(raw, dict) else ():
         try:
             shape = BlockShape(int(v["item_groups"]), int(v["tile_width"]),
-                               None if v.get("us_per_step") is None else float(v["us_per_step"]))
+                               None if v.get("us_per_step") is None else float(v["us_per_step"]),
+                               bool(v.get("node_tiles", False)))
         except (KeyError, TypeError, ValueError):
             continue
-        if shape.item_groups >= 1 and shape.tile_width in PANELS:
+        if shape.item_groups >= 1 and shape.tile_width in PANELS and not (
+                shape.node_tiles and shape.item_groups % TILE_GROUPS):
             out[key] = shape
     return out
 
@@ -210,9 +232,10 @@ def save_tuning(key, shape, path=None):
     """Merge one entry into the cache file (written to a temporary file and renamed, so a
     concurrent reader never sees a partial file)."""
     path = path or tuning_cache_path()
-    entries = {k: {"item_groups": s.item_groups, "tile_width": s.tile_width, "us_per_step": s.us_per_step}
-               for k, s in load_tuning(path).items()}
-    entries[key] = {"item_groups": shape.item_groups, "tile_width": shape.tile_width, "us_per_step": shape.us_per_step}
+    entries = {k: {"item_groups": s.item_groups, "tile_width": s.tile_width, "us_per_step": s.us_per_step,
+                   "node_tiles": s.node_tiles} for k, s in load_tuning(path).items()}
+    entries[key] = {"item_groups": shape.item_groups, "tile_width": shape.tile_width,
+                    "us_per_step": shape.us_per_step, "node_tiles": shape.node_tiles}
     try:
         os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
         fd, tmp = tempfile.mkstemp(dir=os.path.dirname(path) or ".", suffix=".tmp")
@@ -223,7 +246,7 @@ def save_tuning(key, shape, path=None):
         pass                   # a read-only home directory keeps the in-process cache only
 
 
-def _step_cost_us(op, items, B_panel, cols, precision, short=4, long=20):
+def _step_cost_us(op, items, B_panel, cols, precision, short=4, long=20, problem_groups=None):
     """Device time of one block-PCG step over this panel: two runs of tol 0 (no column
     converges) of `short` and `long` steps, timed with CUDA events; the difference over
     long - short removes setup and graph capture."""
@@ -231,7 +254,7 @@ def _step_cost_us(op, items, B_panel, cols, precision, short=4, long=20):
     for steps in (short, long, short, long):
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record()
-        _block_pcg_call(op, *items, B_panel, cols, 0.0, steps, precision, 0.1, 8)
+        _block_pcg_call(op, *items, B_panel, cols, 0.0, steps, precision, 0.1, 8, problem_groups)
         b.record()
         b.synchronize()
         times.append(a.elapsed_time(b) * 1e3)
@@ -239,9 +262,10 @@ def _step_cost_us(op, items, B_panel, cols, precision, short=4, long=20):
 
 
 def tuned_block_shape(op, row_bounds, B_panel, cols, precision="fp64", candidates=None):
-    """The (work-item groups, column tile width) with the cheapest measured block-PCG step for
-    this operator and panel, timed on the actual operator and right-hand sides over
-    ITEM_GROUPS x {panel widths <= K}; a tile narrower than K costs K / width tile steps.
+    """The (work-item groups, column tile width, node tiles or single row groups) with the
+    cheapest measured block-PCG step for this operator and panel, timed on the actual operator
+    and right-hand sides over ITEM_GROUPS x {panel widths <= K} x {node tiles, row groups}; a
+    tile narrower than K costs K / width tile steps.
     Cached in this process and in the JSON file of tuning_cache_path(), keyed by (GPU, n, nnz,
     problems, K, precision)."""
     n, K = B_panel.shape
@@ -257,14 +281,16 @@ def tuned_block_shape(op, row_bounds, B_panel, cols, precision="fp64", candidate
     gp = op.pattern.group_ptr.cpu().numpy()
     cols = np.asarray(cols, np.int64)
     if candidates is None:
-        candidates = [(g, w) for g in ITEM_GROUPS for w in PANELS if 16 <= w <= K or w == K]
+        candidates = [(g, w, nt) for g in ITEM_GROUPS for w in PANELS if 16 <= w <= K or w == K
+                      for nt in (False, True) if not (nt and g % TILE_GROUPS)]
     best = None
-    for g, w in candidates:
+    for g, w, nt in candidates:
         items = _work_items(gp, np.asarray(row_bounds), g)
         ct = np.clip(cols, 0, w)
-        cost = _step_cost_us(op, items, B_panel[:, :w].contiguous(), ct, precision) * (K // w)
+        pgroups = _problem_groups(gp, np.asarray(row_bounds)) if nt else None
+        cost = _step_cost_us(op, items, B_panel[:, :w].contiguous(), ct, precision, problem_groups=pgroups) * (K // w)
         if best is None or cost < best.us_per_step:
-            best = BlockShape(g, w, cost)
+            best = BlockShape(g, w, cost, nt)
     _tuned_block[key] = best
     save_tuning(key, best)
     return best

@@ -79,6 +79,7 @@ class ReducedOperator:
     dinv32: torch.Tensor | None
     _diff: object = None
     _sell: dict = None
+    _tiles: dict = None
 
     def diff_operator(self):
         """The difference-form operator of the mixed block-PCG (7-byte values, 44-bit mantissas;
@@ -98,6 +99,39 @@ class ReducedOperator:
             L.raise_for(rc, "difference-form operator")
             self._diff = (storage, d)
         return self._diff[1]
+
+    def tile_operator(self, precision="fp64", problem_groups=None):
+        """Node tiles of the block SpMM (feab_tile_operator_build): FEAB_TILE_GROUPS consecutive
+        row groups whose column lists are merged, with "fp64" (CSR) or "mixed" (difference-form,
+        44-bit) values.  Tiles never cross the boundaries in problem_groups (the first row group
+        of each problem, then n_groups; default one problem).  Cached per (precision, boundaries)."""
+        if precision not in ("fp64", "mixed"):
+            raise ValueError("the tile operator holds 'fp64' or 'mixed' values")
+        p = self.pattern
+        if p.group_ptr is None:
+            raise ValueError("the tile operator needs node row groups (an assembled K_ff)")
+        pg = np.asarray([0, p.n_groups] if problem_groups is None else problem_groups, dtype=np.int32)
+        key = (precision, pg.tobytes())
+        if self._tiles is None:
+            self._tiles = {}
+        if key not in self._tiles:
+            dev = self.vals64.device
+            pg_t = torch.as_tensor(pg).to(dev)
+            n_prob = len(pg) - 1
+            diff = C.byref(self.diff_operator()) if precision == "mixed" else None
+            sbytes = int(L.lib.feab_tile_scratch_bytes(p.n_groups, n_prob))
+            scratch = torch.empty(max(sbytes, 1), dtype=torch.uint8, device=dev)
+            csr = self.csr_struct()
+            need = C.c_size_t(0)
+            args = (C.byref(csr), diff, L.dptr(pg_t), n_prob, PRECISIONS[precision], L.dptr(scratch), sbytes)
+            L.raise_for(L.lib.feab_tile_operator_build(*args, None, 0, C.byref(need), None, L.stream_ptr(dev)),
+                        "tile operator")
+            storage = torch.empty(need.value, dtype=torch.uint8, device=dev)
+            t = L.TileOperator()
+            L.raise_for(L.lib.feab_tile_operator_build(*args, L.dptr(storage), need.value, None, C.byref(t),
+                                                       L.stream_ptr(dev)), "tile operator")
+            self._tiles[key] = (storage, t)
+        return self._tiles[key][1]
 
     def max_row_len(self):
         rp = self.pattern.row_ptr

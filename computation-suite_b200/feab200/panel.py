@@ -24,15 +24,17 @@ def _f64_panel(X, what):
     return X
 
 
-def block_spmm(op: ReducedOperator, X, out=None):
-    """K X for an (n, k) device panel, k a power of two <= 64."""
+def block_spmm(op: ReducedOperator, X, out=None, node_tiles=True):
+    """K X for an (n, k) device panel, k a power of two <= 64 (through the operator's node tiles,
+    ``ReducedOperator.tile_operator``, unless node_tiles is false)."""
     X = _f64_panel(X, "X").contiguous()
     n, k = X.shape
     if n != op.n or k not in WIDTHS:
         raise ValueError(f"block_spmm: X must be ({op.n}, k) with k in {WIDTHS}, got {tuple(X.shape)}")
     Y = out if out is not None else torch.empty_like(X)
     csr = op.csr_struct()
-    rc = L.lib.feab_block_spmm(C.byref(csr), L.dptr(X), L.dptr(Y), k, L.stream_ptr(X.device))
+    tiles = C.byref(op.tile_operator("fp64")) if node_tiles else None
+    rc = L.lib.feab_block_spmm(C.byref(csr), tiles, L.dptr(X), L.dptr(Y), k, L.stream_ptr(X.device))
     L.raise_for(rc, "block_spmm")
     return Y
 

@@ -329,16 +329,74 @@ typedef struct feab_batch {
 
 size_t feab_block_pcg_workspace_bytes(int32_t n, int32_t k, int32_t n_problems, int32_t n_items);
 
-int32_t feab_block_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const feab_batch* batch,
-                             const double* dinv64, const double* B, double* X, const feab_pcg_params* params,
-                             void* workspace, size_t workspace_bytes, int32_t* iters_out, double* relres_out,
-                             int32_t* status_out, cudaStream_t stream);
+/* ---------------------------------------------------------------- node tiles of the block SpMM
+ * FEAB_TILE_GROUPS consecutive node row groups of one problem form a tile, which one warp
+ * applies: it walks the union of the tiles' column lists and gathers each panel row once for
+ * every group of the tile that has the column (consecutive nodes of a structured hex8 mesh share
+ * 2/3 of their neighbours, so a 4-group tile gathers half the panel rows its groups would gather
+ * one by one).  Tile t covers groups tile_g0[t] .. tile_g0[t+1]-1 (tiles start at each problem's
+ * first group and every FEAB_TILE_GROUPS groups after it); its union columns are
+ * ucol[uoff[t] .. uoff[t+1]), grouped by mask (every column of mask 1, then of mask 2, ...,
+ * ascending within a mask), padded to a multiple of 4 with mask 0; bit j of umask[u] says that
+ * group tile_g0[t] + j has column ucol[u].  Values follow in the same order:
+ * from value 3 * poff[t], for each union column, for each set bit j ascending, rows 0..2 of group
+ * tile_g0[t] + j (rows past the group's free DOFs are 0).  FEAB_PREC_FP64: the CSR's FP64 values
+ * (own-node columns included) in v64.  FEAB_PREC_MIXED: the feab_diff_operator's off-node columns
+ * and 44-bit values in vhi / vlo / vlo2 (the own-node term comes from that operator's S). */
+#define FEAB_TILE_GROUPS 4
+#define FEAB_TILE_CHUNK 64   /* union columns the SpMM stages at a time */
+
+typedef struct feab_tile_operator {
+  int32_t n_tiles;
+  int32_t precision;     /* FEAB_PREC_FP64 or FEAB_PREC_MIXED                         */
+  int32_t n_groups;
+  int32_t reserved;
+  int32_t* tile_g0;      /* n_tiles + 1: first row group of each tile                  */
+  int32_t* group_tile;   /* n_groups: tile of each row group                           */
+  int32_t* uoff;         /* n_tiles + 1: first union column (a multiple of 4)          */
+  int32_t* poff;         /* n_tiles + 1: first (column, group) pair                    */
+  int32_t* ucol;         /* union columns                                              */
+  int32_t* upair;        /* per union column: its first pair within the tile           */
+  uint8_t* umask;        /* per union column: the groups of the tile that have it      */
+  double* v64;           /* FEAB_PREC_FP64: 3 values per pair                          */
+  uint32_t* vhi;         /* FEAB_PREC_MIXED: 3 values per pair, 44-bit as in           */
+  uint16_t* vlo;         /*   feab_diff_operator                                       */
+  uint8_t* vlo2;
+  int32_t* cptr;         /* n_tiles + 1: first chunk of each tile                      */
+  int32_t* chunk;        /* 4 per chunk (FEAB_TILE_CHUNK union columns of a tile):     */
+                         /*   first union column, columns, first value, values        */
+} feab_tile_operator;
+
+/* Scratch for feab_tile_operator_build. */
+size_t feab_tile_scratch_bytes(int32_t n_groups, int32_t n_problems);
+
+/* Tiles of A's node row groups (A needs group_ptr), never crossing a problem boundary:
+ * problem_groups (device, n_problems + 1) are the first row group of each problem and n_groups.
+ * precision FEAB_PREC_MIXED needs diff (built from A).  Call with storage == NULL to get
+ * *bytes_out (synchronous: the unions are counted on the device), then again with that much
+ * storage (16-byte aligned) to build *out (synchronous).  Needs fewer than 2^31 union columns
+ * and 2^31 values. */
+int32_t feab_tile_operator_build(const feab_csr* A, const feab_diff_operator* diff, const int32_t* problem_groups,
+                                 int32_t n_problems, int32_t precision, void* scratch, size_t scratch_bytes,
+                                 void* storage, size_t storage_bytes, size_t* bytes_out, feab_tile_operator* out,
+                                 cudaStream_t stream);
+
+/* tiles (optional, of the solve's precision, built with this batch's problem boundaries): the
+ * SpMM of every CG step walks node tiles instead of single row groups; work items must then
+ * start and end on tile boundaries (items of a multiple of FEAB_TILE_GROUPS groups from each
+ * problem's first group do).  The mixed solve's FP64 residual replacements use A and diff. */
+int32_t feab_block_pcg_solve(const feab_csr* A, const feab_diff_operator* diff, const feab_tile_operator* tiles,
+                             const feab_batch* batch, const double* dinv64, const double* B, double* X,
+                             const feab_pcg_params* params, void* workspace, size_t workspace_bytes,
+                             int32_t* iters_out, double* relres_out, int32_t* status_out, cudaStream_t stream);
 
 /* Y = A X for a row-major n x k panel X (k in {1,2,4,8,16,32,64}; X 16-byte aligned for
  * k = 64): the block-PCG's SpMM on the plain CSR (FP64 values, node row groups required) on its
- * own.  Applies K_ff or M_ff to the whole block of vectors of the modal subspace iteration (the
- * products eigsh makes inside FESystem.solve_modal, solver.py:2047-2114).  Asynchronous. */
-int32_t feab_block_spmm(const feab_csr* A, const double* X, double* Y, int32_t k, cudaStream_t stream);
+ * own, through the node tiles when tiles (FEAB_PREC_FP64) is given.  Applies K_ff or M_ff to the
+ * whole block of vectors of the modal subspace iteration (the products eigsh makes inside
+ * FESystem.solve_modal, solver.py:2047-2114).  Asynchronous. */
+int32_t feab_block_spmm(const feab_csr* A, const feab_tile_operator* tiles, const double* X, double* Y, int32_t k,
+                        cudaStream_t stream);
 
 /* ---------------------------------------------------------------- POD Gram + eigensolve
  * Replaces the FP64 economy SVD of PodBasis._fit_standard (rom_engine/src/rom_engine/pod.py:

@@ -15,17 +15,18 @@ def _operator(shape=(10, 3, 3)):
     return dm.assemble(dm.element_stiffness(c.D), dm.pattern(c.fixed), want32=False)
 
 
-@pytest.mark.parametrize("k", [1, 4, 16, 64])
-def test_block_spmm_matches_csr_product(k):
+@pytest.mark.parametrize("node_tiles", [True, False])
+@pytest.mark.parametrize("k", [1, 4, 16, 32, 64])
+def test_block_spmm_matches_csr_product(k, node_tiles):
     from feab200.panel import block_spmm
     op = _operator()
     A = torch.sparse_csr_tensor(op.pattern.row_ptr.long(), op.pattern.col_idx.long(), op.vals64, size=(op.n, op.n))
     X = torch.as_tensor(np.random.default_rng(k).standard_normal((op.n, k))).cuda()
-    Y = block_spmm(op, X)
+    Y = block_spmm(op, X, node_tiles=node_tiles)
     ref = (A @ X)
     assert float(torch.linalg.norm(Y - ref) / torch.linalg.norm(ref)) < 1e-14
     # deterministic: the same bits on a second call
-    assert torch.equal(block_spmm(op, X), Y)
+    assert torch.equal(block_spmm(op, X, node_tiles=node_tiles), Y)
 
 
 @pytest.mark.parametrize("k", [1, 7, 16, 64])

@@ -179,14 +179,15 @@ def test_block_tuning_cache_round_trip(tmp_path):
     k2 = bt.tuning_key("NVIDIA B200", 418176, 32348142, 1, 64, "mixed")
     assert k1 != k2
     bt.save_tuning(k1, bt.BlockShape(32, 64, 512.5), path)
-    bt.save_tuning(k2, bt.BlockShape(128, 32, 480.0), path)
+    bt.save_tuning(k2, bt.BlockShape(128, 32, 480.0, True), path)
     got = bt.load_tuning(path)
-    assert got == {k1: bt.BlockShape(32, 64, 512.5), k2: bt.BlockShape(128, 32, 480.0)}
+    assert got == {k1: bt.BlockShape(32, 64, 512.5), k2: bt.BlockShape(128, 32, 480.0, True)}
     # malformed entries are ignored, a missing or corrupt file reads as empty
     import json
     raw = json.load(open(path))
     raw["bad"] = {"item_groups": 0, "tile_width": 64}
     raw["worse"] = {"tile_width": 3}
+    raw["tiles_on_ragged_items"] = {"item_groups": 6, "tile_width": 64, "node_tiles": True}
     json.dump(raw, open(path, "w"))
     assert set(bt.load_tuning(path)) == {k1, k2}
     open(path, "w").write("{not json")

@@ -48,6 +48,24 @@
 #ifndef FEAB_SELL_MINB_MIXED
 #define FEAB_SELL_MINB_MIXED 4
 #endif
+// 1: software pipelining, one block of 4 steps: a lane issues the loads of block i + 1 before the
+// gathers and products of block i, so the operator's DRAM latency overlaps the gathers' L2
+// latency (per operator kind; replaces FEAB_SELL_BLOCKS_* and uses FEAB_SELL_PIPE_MINB_*).
+// Measured in the PCG at 128x32x32 and left off: the second block's registers (80 for the 48-bit
+// kernel, 3 CTAs per SM; 98 for FP64) cost more warps than the overlap gains, 63.9 against 51.8 us
+// per iteration (mixed) and 62.4 against 59.4 us (FP64).
+#ifndef FEAB_SELL_PIPE_FP64
+#define FEAB_SELL_PIPE_FP64 0
+#endif
+#ifndef FEAB_SELL_PIPE_MIXED
+#define FEAB_SELL_PIPE_MIXED 0
+#endif
+#ifndef FEAB_SELL_PIPE_MINB_FP64
+#define FEAB_SELL_PIPE_MINB_FP64 2
+#endif
+#ifndef FEAB_SELL_PIPE_MINB_MIXED
+#define FEAB_SELL_PIPE_MINB_MIXED 3
+#endif
 
 namespace feab {
 
@@ -101,9 +119,84 @@ __device__ __forceinline__ double sell_dec48(uint32_t hi, uint16_t lo) {
 // Per-kind load depth and register budget of the sliced SpMV kernels.
 template <int KIND>
 struct SellTuning {
+  static constexpr bool kPipe = KIND == FEAB_PREC_FP64 ? FEAB_SELL_PIPE_FP64 != 0 : FEAB_SELL_PIPE_MIXED != 0;
   static constexpr int kBlocks = KIND == FEAB_PREC_FP64 ? FEAB_SELL_BLOCKS_FP64 : FEAB_SELL_BLOCKS_MIXED;
-  static constexpr int kMinBlocks = KIND == FEAB_PREC_FP64 ? FEAB_SELL_MINB_FP64 : FEAB_SELL_MINB_MIXED;
+  static constexpr int kMinBlocks =
+      kPipe ? (KIND == FEAB_PREC_FP64 ? FEAB_SELL_PIPE_MINB_FP64 : FEAB_SELL_PIPE_MINB_MIXED)
+            : (KIND == FEAB_PREC_FP64 ? FEAB_SELL_MINB_FP64 : FEAB_SELL_MINB_MIXED);
 };
+
+// One block of 4 steps of a lane: its columns and its rows' values as loaded.
+template <int KIND>
+struct SellBlock {
+  unsigned t[4];
+  double v[KIND == FEAB_PREC_FP64 ? 3 : 1][4];
+  uint4 h[KIND == FEAB_PREC_FP64 ? 1 : 3];
+  uint2 l[KIND == FEAB_PREC_FP64 ? 1 : 3];
+};
+
+// Issues the loads of the block starting at step b (columns decoded to absolute indices; the
+// difference form's tag bits masked off).
+template <int KIND, bool IDX16>
+__device__ __forceinline__ void sell_load_block(const SellView& V, size_t b, int lane, int r0, SellBlock<KIND>& B) {
+  if (IDX16) {
+    const uint2 tq = ld_op(reinterpret_cast<const uint2*>(V.tcol16 + b * 32) + lane);
+    B.t[0] = (unsigned)(r0 + (int)(int16_t)(tq.x & 0xffffu));
+    B.t[1] = (unsigned)(r0 + (int)(int16_t)(tq.x >> 16));
+    B.t[2] = (unsigned)(r0 + (int)(int16_t)(tq.y & 0xffffu));
+    B.t[3] = (unsigned)(r0 + (int)(int16_t)(tq.y >> 16));
+  } else {
+    const uint4 tq = ld_op(reinterpret_cast<const uint4*>(V.tcol + b * 32) + lane);
+    const unsigned m = KIND == FEAB_PREC_FP64 ? 0xffffffffu : 0x3fffffffu;
+    B.t[0] = tq.x & m;
+    B.t[1] = tq.y & m;
+    B.t[2] = tq.z & m;
+    B.t[3] = tq.w & m;
+  }
+  if (KIND == FEAB_PREC_FP64) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double2* vp = reinterpret_cast<const double2*>(V.v64 + (3 * b + 4 * k) * 32) + 2 * lane;
+      const double2 p0 = ld_op(vp), p1 = ld_op(vp + 1);
+      B.v[k][0] = p0.x;
+      B.v[k][1] = p0.y;
+      B.v[k][2] = p1.x;
+      B.v[k][3] = p1.y;
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const size_t o = (3 * b + 4 * k) * 32;
+      B.h[k] = ld_op(reinterpret_cast<const uint4*>(V.vhi + o) + lane);
+      B.l[k] = ld_op(reinterpret_cast<const uint2*>(V.vlo + o) + lane);
+    }
+  }
+}
+
+// a_k += sum_u value(k, u) d[u] over the block's 4 steps.
+template <int KIND>
+__device__ __forceinline__ void sell_use_block(const SellBlock<KIND>& B, const double (&d)[4], double& a0,
+                                               double& a1, double& a2) {
+  if (KIND == FEAB_PREC_FP64) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      a0 = fma(B.v[0][u], d[u], a0);
+      a1 = fma(B.v[1][u], d[u], a1);
+      a2 = fma(B.v[2][u], d[u], a2);
+    }
+  } else {
+    double* acc[3] = {&a0, &a1, &a2};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double a = *acc[k];
+      a = fma(sell_dec48(B.h[k].x, (uint16_t)(B.l[k].x & 0xffffu)), d[0], a);
+      a = fma(sell_dec48(B.h[k].y, (uint16_t)(B.l[k].x >> 16)), d[1], a);
+      a = fma(sell_dec48(B.h[k].z, (uint16_t)(B.l[k].y & 0xffffu)), d[2], a);
+      a = fma(sell_dec48(B.h[k].w, (uint16_t)(B.l[k].y >> 16)), d[3], a);
+      *acc[k] = a;
+    }
+  }
+}
 
 // acc[k] = (K x)[r0 + k] for the lane's group, x read through xf(column).  Mixed kind: the
 // difference form sum_{b != a} w (x_b - x_a) + S x_a, evaluated as sum_{b != a} w x_b + T x_a
@@ -135,6 +228,19 @@ __device__ __forceinline__ void sell_apply(const SellView& V, int slice, int lan
   };
 #pragma unroll
   for (int i = 1; i < FEAB_SELL_PREFETCH; ++i) prefetch_block(4 * i);
+  if constexpr (SellTuning<KIND>::kPipe) {
+    // block i + 1's loads are in flight while block i's gathers and products run
+    SellBlock<KIND> cur, nxt;
+    if (W > 0) sell_load_block<KIND, IDX16>(V, (size_t)base, lane, L.r0, cur);
+    for (int j = 0; j < W; j += 4) {
+      if (j + 4 < W) sell_load_block<KIND, IDX16>(V, (size_t)(base + j + 4), lane, L.r0, nxt);
+      double d[4];
+#pragma unroll
+      for (int u = 0; u < 4; ++u) d[u] = xf((int)cur.t[u]);
+      sell_use_block<KIND>(cur, d, a0, a1, a2);
+      cur = nxt;
+    }
+  } else
   for (int j = 0; j < W; j += 4 * NB) {
     prefetch_block(j + 4 * FEAB_SELL_PREFETCH);
     // all loads of NB blocks first (a block past the slice end is skipped; W is

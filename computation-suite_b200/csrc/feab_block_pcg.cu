@@ -155,7 +155,22 @@ constexpr int kVecU = FEAB_BLOCK_VECU;
 // own-node term push it past the 128 registers of two CTAs per SM); measured at 128x32x32 with
 // 64 columns: 1078 -> 1003 us per FP64 step
 constexpr int kUnrollFp64 = 16;
-static_assert(kStageCols % kUnrollFp64 == 0 && kStageCols % kUnroll == 0, "vector reads stay inside the stage");
+// The group-path SpMM (kernel A when the operator has no node tiles, and the stand-alone block
+// SpMM) is bound by the L1 data path (each 512-byte panel-row gather is four wavefronts, each
+// value broadcast one); it runs at FEAB_BLOCK_GROUP_MINB resident CTAs per SM with
+// FEAB_BLOCK_GROUP_UNROLL gathers in flight per lane, so that more warps hide the gathers'
+// latency.  Measured at 128x32x32 with 64 columns (FP64 SpMM, L2 flushed): 4 CTAs and 8 gathers
+// 386 us, 4 and 4 401 us, 3 and 8 434 us, 2 and 16 475 us (a few spilled registers at 4 CTAs and
+// 8 gathers cost less than the occupancy gains).
+#ifndef FEAB_BLOCK_GROUP_MINB
+#define FEAB_BLOCK_GROUP_MINB 4
+#endif
+#ifndef FEAB_BLOCK_GROUP_UNROLL
+#define FEAB_BLOCK_GROUP_UNROLL 8
+#endif
+constexpr int kGroupU = FEAB_BLOCK_GROUP_UNROLL;
+static_assert(kStageCols % kUnrollFp64 == 0 && kStageCols % kUnroll == 0 && kStageCols % kGroupU == 0,
+              "vector reads stay inside the stage");
 
 struct __align__(16) GroupStage {
   int col[kStageCols];
@@ -660,15 +675,19 @@ __global__ void __launch_bounds__(kThreads) k_bsetup(BArgs A) {
 }
 
 // Step A: AP = K P (P updated by k_bstep_p; or, in a reliable step, R = B - K64 X);
-// per-column partial p.Ap (or r.r).
-template <int K, bool MIXED>
-__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) {
+// per-column partial p.Ap (or r.r).  TILES: the operator has node tiles (the CG steps walk them;
+// a reliable step walks the row groups); otherwise every step walks the row groups, at the
+// group path's occupancy and with a group-sized stage.
+template <int K, bool MIXED, bool TILES>
+__global__ void __launch_bounds__(kThreads, TILES ? FEAB_BLOCK_MINB : FEAB_BLOCK_GROUP_MINB) k_bstep_a(BArgs A) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
   __shared__ double sm[kWarps][K];
-  extern __shared__ __align__(16) unsigned char dyn_stage[];  // one WarpStage per warp
+  // one stage per warp: a WarpStage with tiles, a GroupStage without
+  extern __shared__ __align__(16) unsigned char dyn_stage[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-  WarpStage& stage = reinterpret_cast<WarpStage*>(dyn_stage)[w];
+  GroupStage& gstage =
+      TILES ? reinterpret_cast<WarpStage*>(dyn_stage)[w].g : reinterpret_cast<GroupStage*>(dyn_stage)[w];
   for (int it = blockIdx.x; it < A.n_items; it += gridDim.x) {
     const int p = A.item_problem[it];
     const ProbState P = A.ps[p];
@@ -696,12 +715,12 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
         }
       }
     };
-    if (A.t_g0 && !reliable) {
+    if (TILES && !reliable) {
       int t0, t1;
       item_tiles(A, it, t0, t1);
       for (int t = t0 + w; t < t1; t += kWarps) {
         double acc[kTG][3][CPL];
-        tile_spmm<K, MIXED>(A, t, lane, stage.t, po, acc);
+        tile_spmm<K, MIXED>(A, t, lane, reinterpret_cast<WarpStage*>(dyn_stage)[w].t, po, acc);
         if (lane < LW) {
           const int tg0 = A.t_g0[t], nt = A.t_g0[t + 1] - tg0;
 #pragma unroll
@@ -721,10 +740,10 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_bstep_a(BArgs A) 
       for (int g = A.item_g0[it] + w; g < g1; g += kWarps) {
         double acc[3][CPL];
         if constexpr (MIXED) {
-          if (!diff) group_spmm<K, false>(A, g, lane, stage.g, src, acc);
-          else group_spmm<K, true>(A, g, lane, stage.g, po, acc);
+          if (!diff) group_spmm<K, false, TILES ? kUnroll : kGroupU>(A, g, lane, gstage, src, acc);
+          else group_spmm<K, true, TILES ? kUnroll : kGroupU>(A, g, lane, gstage, po, acc);
         } else {
-          group_spmm<K, false, kUnrollFp64>(A, g, lane, stage.g, po, acc);
+          group_spmm<K, false, TILES ? kUnrollFp64 : kGroupU>(A, g, lane, gstage, po, acc);
         }
         if (lane < LW) {
           const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
@@ -1050,15 +1069,15 @@ __global__ void __launch_bounds__(kThreads, FEAB_BLOCK_B_MINB) k_bstep_b(BArgs A
 // Y = K X for a whole n x K panel (the plain CSR, FP64 values): the SpMM of step A on its own,
 // one warp per node row group, grid-stride over the groups.
 template <int K>
-__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_MINB) k_block_spmm(BArgs A, const double* __restrict__ src,
-                                                                         double* __restrict__ dst) {
+__global__ void __launch_bounds__(kThreads, FEAB_BLOCK_GROUP_MINB) k_block_spmm(BArgs A, const double* __restrict__ src,
+                                                                               double* __restrict__ dst) {
   constexpr int CPL = K >= 32 ? K / 32 : 1;
   constexpr int LW = K >= 32 ? 32 : K;
   __shared__ GroupStage stage[kWarps];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   for (int g = blockIdx.x * kWarps + w; g < A.n_groups; g += gridDim.x * kWarps) {
     double acc[3][CPL];
-    group_spmm<K, false, kUnrollFp64>(A, g, lane, stage[w], src, acc);
+    group_spmm<K, false, kGroupU>(A, g, lane, stage[w], src, acc);
     if (lane < LW) {
       const int r0 = A.group_ptr[g], f = A.group_ptr[g + 1] - r0;
 #pragma unroll
@@ -1169,24 +1188,30 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   };
   do {
     if (fail(graphs.events(ev))) break;
-    const size_t smem_a = kStageBytes;
-    if (fail(cudaFuncSetAttribute(k_bstep_a<K, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
-    if (fail(cudaFuncSetAttribute(k_bstep_a<K, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_a))) break;
+    const bool tiles = A.t_g0 != nullptr;
+    const size_t smem_a = tiles ? kStageBytes : kWarps * sizeof(GroupStage);
+    if (fail(cudaFuncSetAttribute(k_bstep_a<K, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kStageBytes)))
+      break;
+    if (fail(cudaFuncSetAttribute(k_bstep_a<K, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kStageBytes)))
+      break;
     auto record = [&](cudaStream_t cs) {
       for (int q = 0; q < chunk; ++q) {
+        k_bstep_p<K><<<grid_pb, kThreads, 0, cs>>>(A);
         if (prec == FEAB_PREC_MIXED) {
-          k_bstep_p<K><<<grid_pb, kThreads, 0, cs>>>(A);
-          k_bstep_a<K, true><<<grid, kThreads, smem_a, cs>>>(A);
+          if (tiles) k_bstep_a<K, true, true><<<grid, kThreads, smem_a, cs>>>(A);
+          else k_bstep_a<K, true, false><<<grid, kThreads, smem_a, cs>>>(A);
           k_bstep_b<K, true><<<grid_pb, kThreads, 0, cs>>>(A);
         } else {
-          k_bstep_p<K><<<grid_pb, kThreads, 0, cs>>>(A);
-          k_bstep_a<K, false><<<grid, kThreads, smem_a, cs>>>(A);
+          if (tiles) k_bstep_a<K, false, true><<<grid, kThreads, smem_a, cs>>>(A);
+          else k_bstep_a<K, false, false><<<grid, kThreads, smem_a, cs>>>(A);
           k_bstep_b<K, false><<<grid_pb, kThreads, 0, cs>>>(A);
         }
       }
       cudaMemcpyAsync((void*)hflag, A.remaining, sizeof(int32_t), cudaMemcpyDeviceToHost, cs);
     };
-    if (fail(graphs.acquire(&A, sizeof(A), topo_signature({K, prec, chunk, grid, grid_pb}), record, &exec))) break;
+    if (fail(graphs.acquire(&A, sizeof(A), topo_signature({K, prec, chunk, grid, grid_pb, tiles ? 1 : 0}), record, &exec))) break;
     // iterations and reliable steps per problem are bounded by maxiter each
     const int64_t max_launch = (2 * (int64_t)maxiter + 2 + chunk - 1) / chunk + 1;
     hflag[0] = np;

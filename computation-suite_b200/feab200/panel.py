@@ -24,9 +24,10 @@ def _f64_panel(X, what):
     return X
 
 
-def block_spmm(op: ReducedOperator, X, out=None, node_tiles=True):
-    """K X for an (n, k) device panel, k a power of two <= 64 (through the operator's node tiles,
-    ``ReducedOperator.tile_operator``, unless node_tiles is false)."""
+def block_spmm(op: ReducedOperator, X, out=None, node_tiles=False):
+    """K X for an (n, k) device panel, k a power of two <= 64: one warp per node row group at
+    four resident CTAs per SM (the faster form at every size measured), or, with node_tiles,
+    through the operator's node tiles (``ReducedOperator.tile_operator``)."""
     X = _f64_panel(X, "X").contiguous()
     n, k = X.shape
     if n != op.n or k not in WIDTHS:

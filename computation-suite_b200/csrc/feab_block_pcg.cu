@@ -1175,8 +1175,9 @@ int32_t run_block(BArgs A, int prec, int chunk, int maxiter, cudaStream_t s, int
   k_bsetup<K><<<grid, kThreads, 0, s>>>(A);
   count_launches(1);
   if (cudaGetLastError() != cudaSuccess) return FEAB_CUDA_ERROR;
-  static thread_local HostFlag flag;
-  static thread_local GraphCache graphs;
+  SolverState& state = thread_solver_state<1>();
+  HostFlag& flag = state.flag;
+  GraphCache& graphs = state.graphs;
   if (!flag.ptr) return FEAB_CUDA_ERROR;
   volatile int32_t* hflag = flag.ptr;
   cudaGraphExec_t exec = nullptr;

@@ -160,6 +160,24 @@ class GraphCache {
   uint64_t clock_ = 0;
 };
 
+// Per-thread solver state: the pinned done flag and the graph cache.  It is created on a thread's
+// first solve and deliberately never destroyed.  Destructors that run at thread or process exit
+// would make CUDA calls while the CUDA runtime may already be shutting down (process exit), which
+// can crash the exiting process after all its work is done.  So a thread that has solved keeps a
+// 64-byte pinned word, at most kSlots graph executables, two events and one capture stream per
+// device until the process ends.  ID separates the single- and multi-right-hand-side solvers.
+struct SolverState {
+  HostFlag flag;
+  GraphCache graphs;
+};
+
+template <int ID>
+inline SolverState& thread_solver_state() {
+  static thread_local SolverState* state = nullptr;  // trivially destructible: no exit-time work
+  if (!state) state = new SolverState();
+  return *state;
+}
+
 // FNV-1a over a few integers: the topology signature of a captured chunk.
 inline uint64_t topo_signature(std::initializer_list<int64_t> v) {
   uint64_t h = 1469598103934665603ull;

@@ -843,14 +843,15 @@ int normalize_lpg(int lpg) { return lpg == 4 || lpg == 8 || lpg == 16 || lpg == 
 int32_t run_pcg(const PcgArgs& A, int prec, int chunk, int maxiter, int lpg, feab_pcg_result* result,
                 cudaStream_t s) {
   const Grids gr = grids_for(A.n, A.group_ptr ? A.n_groups : A.n);
-  static thread_local HostFlag flag;
+  SolverState& state = thread_solver_state<0>();
+  HostFlag& flag = state.flag;
   if (!flag.ptr) return FEAB_CUDA_ERROR;
   if (prec == FEAB_PREC_FP32) launch_setup<FEAB_PREC_FP32>(A, gr, lpg, s);
   else if (prec == FEAB_PREC_MIXED) launch_setup<FEAB_PREC_MIXED>(A, gr, lpg, s);
   else launch_setup<FEAB_PREC_FP64>(A, gr, lpg, s);
   FEAB_CHECK_LAUNCH();
 
-  static thread_local GraphCache graphs;
+  GraphCache& graphs = state.graphs;
   cudaGraphExec_t exec = nullptr;
   cudaEvent_t ev[2] = {nullptr, nullptr};
   int32_t rc = FEAB_OK;

@@ -257,18 +257,30 @@ class DeviceMesh:
         fm[mask] = np.arange(int(mask.sum()), dtype=np.int32)
         return fm
 
+    def _fixed_set(self, fixed_dofs):
+        """The fixed DOFs as a sorted, duplicate-free int64 array (range-checked)."""
+        fixed = np.unique(np.asarray(fixed_dofs, dtype=np.int64).reshape(-1))
+        if fixed.size and (fixed[0] < 0 or fixed[-1] >= 3 * self.n_nodes):
+            raise ValueError("fixed DOF index outside the system")
+        return fixed
+
     def pattern(self, fixed_dofs=()) -> Pattern:
-        fm_host = self.free_map(fixed_dofs)
-        key = hash(fm_host.tobytes())
+        # the free map is a function of the fixed-DOF set alone: the set is the cache key, and the
+        # map is built on the device (no host pass over all DOFs)
+        fixed = self._fixed_set(fixed_dofs)
+        key = fixed.tobytes()
         hit = self._patterns.get(key)
-        if hit is not None and np.array_equal(hit[0], fm_host):
-            return hit[1]
+        if hit is not None:
+            return hit
         topo = self.topology()
         dev, N = self.device, self.n_nodes
-        n_free = int((fm_host >= 0).sum())
+        n_free = 3 * N - int(fixed.size)
         if n_free == 0:
             raise ValueError("every DOF is fixed: the reduced system is empty")
-        free_map = torch.as_tensor(fm_host).to(dev)
+        keep = torch.ones(3 * N, dtype=torch.int32, device=dev)
+        if fixed.size:
+            keep[torch.as_tensor(fixed).to(dev)] = 0
+        free_map = torch.where(keep > 0, torch.cumsum(keep, 0, dtype=torch.int32) - 1, -1).to(torch.int32)
         sbytes = int(L.lib.feab_topology_scratch_bytes(N, self.n_elem))
         scratch = torch.empty(sbytes, dtype=torch.uint8, device=dev)
         row_ptr = torch.empty(n_free + 1, dtype=torch.int32, device=dev)
@@ -285,7 +297,7 @@ class DeviceMesh:
         L.raise_for(rc, "CSR pattern")
         pat = Pattern(n_free, int(nnz.value), int(ng.value), row_ptr, col_idx[: int(nnz.value)],
                       group_ptr[: int(ng.value) + 1], free_map)
-        self._patterns[key] = (fm_host, pat)
+        self._patterns[key] = pat
         return pat
 
     # ------------------------------------------------------------------ element matrices

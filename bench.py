@@ -49,7 +49,7 @@ def parse():
                     help="skip the oracle job (CPU baseline and the full-size accuracy check against the oracle)")
     ap.add_argument("--spmv-reps", type=int, default=20)
     ap.add_argument("--workload", choices=["cantilever", "simp", "batch", "snapshot", "gram", "spmv", "recovery",
-                                           "simp_oc", "elements", "modal", "block_step"],
+                                           "simp_oc", "elements", "modal", "block_step", "direct"],
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
@@ -1041,6 +1041,55 @@ def workload_block_step(args):
             "timing": "step: CUDA events over whole runs; SpMM: CUDA events around each launch, L2 flushed before each"}
 
 
+def workload_direct(args):
+    """The direct solve of solve_static(method=None) (the reference's SuperLU splu,
+    _sparse_lu_solve) as a banded Cholesky on the GPU, on the random-tip cantilever at 64x16x16
+    and at --shape: ordering + band assembly + factorisation, and one solve, with the relative
+    residual and the difference from a Jacobi-PCG solve at 1e-12.  The reference's splu at
+    64x16x16 took 59.6 s on the survey container's 8 cores; at 128x32x32 its fill does not fit."""
+    import torch
+    from feab200 import cantilever
+    from feab200.device import DeviceMesh, pcg_solve, spmv
+    from feab200.direct import BandCholesky
+    out = {}
+    for shape in ((64, 16, 16), tuple(args.shape)):
+        c = cantilever.random_tip_cantilever(*shape)
+        dm = DeviceMesh(c.mesh.nodes, c.mesh.elements)
+        op = dm.assemble(dm.element_stiffness(c.D), dm.pattern(c.fixed), want32=False)
+        b = torch.as_tensor(c.F[c.free]).to(op.vals64.device)
+        fac_ms, solve_ms = [], []
+        for _ in range(max(1, args.steps)):
+            op._direct = None
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            fac = op.direct_factor(coords=c.mesh.nodes)
+            torch.cuda.synchronize()
+            t1 = time.perf_counter()
+            x = fac.solve(b)
+            torch.cuda.synchronize()
+            t2 = time.perf_counter()
+            fac_ms.append(1e3 * (t1 - t0))
+            solve_ms.append(1e3 * (t2 - t1))
+        rel = float(torch.linalg.norm(b - spmv(op, x, lanes_per_group=16)) / torch.linalg.norm(b))
+        xp, info = pcg_solve(op, b, tol=1e-12)
+        nt, nb = fac.band.n_tiles, fac.band.bands
+        gflop = 2 * nt * nb * (nb + 1) / 2 * 64 ** 3 / 1e9            # the trailing updates dominate
+        out["x".join(map(str, shape))] = {
+            "n": op.n, "ordering": fac.ordering, "bandwidth": fac.bandwidth, "band_gb": round(fac.storage.numel() / 1e9, 2),
+            "factor_ms": round(min(fac_ms), 1), "solve_ms": round(min(solve_ms), 1),
+            "update_gflop": round(gflop, 1), "update_tflops": round(gflop / min(fac_ms), 2),
+            "relres": rel, "vs_pcg_1e-12": float(torch.linalg.norm(x - xp) / torch.linalg.norm(xp)),
+            "pivot_ratio": fac.pivots[0] / fac.pivots[1]}
+        del fac, op, dm
+        torch.cuda.empty_cache()
+    key = "x".join(map(str, args.shape))
+    return {"metric": f"direct solve (banded Cholesky) time, {key} cantilever", "value": out[key]["factor_ms"] +
+            out[key]["solve_ms"], "unit": "ms", "cases": out,
+            "timing": "host clock around synchronised calls; factor includes ordering, band assembly and factorisation",
+            "cpu_reference_note": "SuperLU splu (_sparse_lu_solve) at 64x16x16: 59.6 s on the survey container's 8 "
+                                  "cores; infeasible at 128x32x32 (fill)"}
+
+
 class _NoCheck:
     """A device status that is never read back, so a timed element-matrix launch has no sync."""
 
@@ -1136,7 +1185,7 @@ def main():
         fn = {"simp": workload_simp, "batch": workload_batch, "snapshot": workload_snapshot,
               "gram": workload_gram, "spmv": workload_spmv, "recovery": workload_recovery,
               "simp_oc": workload_simp_oc, "elements": workload_elements, "modal": workload_modal,
-              "block_step": workload_block_step}[args.workload]
+              "block_step": workload_block_step, "direct": workload_direct}[args.workload]
         line = fn(args)
         line.update({"n_gpus": world, "steps": args.steps, "warmup": args.warmup, "higher_is_better": False,
                      "data": "synthetic", "workload": args.workload})

@@ -68,6 +68,11 @@ class Batch(C.Structure):
                 ("problem_items", C.c_void_p), ("problem_cols", C.c_void_p)]
 
 
+class Band(C.Structure):
+    _fields_ = [("n", C.c_int32), ("n_tiles", C.c_int32), ("bands", C.c_int32), ("reserved", C.c_int32),
+                ("storage", C.c_void_p)]
+
+
 class PcgParams(C.Structure):
     _fields_ = [("tol", C.c_double), ("maxiter", C.c_int32), ("precision", C.c_int32),
                 ("reliable_delta", C.c_double), ("chunk", C.c_int32), ("use_dinv", C.c_int32),
@@ -137,6 +142,11 @@ SIGNATURES = {
     "feab_oc_update": (_I32, [_P, _P, _I64, _D, _D, _D, _D, _D, _I32, _P, _P, _P, _SZ, _P]),
     "feab_hex8_recover_scratch_bytes": (_SZ, [_I64]),
     "feab_hex8_recover": (_I32, [_P, _P, _I64, _I32, _P, _P, C.POINTER(_D), _P, _P, _P, _P, _P, _P, _SZ, _P, _P]),
+    "feab_band_width": (_I32, [C.POINTER(CSR), _P, _P, C.POINTER(_I32), _P]),
+    "feab_band_bytes": (_SZ, [_I32, _I32]),
+    "feab_band_assemble": (_I32, [C.POINTER(CSR), _P, _I32, C.POINTER(Band), _P]),
+    "feab_band_cholesky": (_I32, [C.POINTER(Band), C.POINTER(_D), _P]),
+    "feab_band_solve": (_I32, [C.POINTER(Band), _P, _P, _P, _P]),
 }
 
 

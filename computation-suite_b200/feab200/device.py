@@ -80,6 +80,15 @@ class ReducedOperator:
     _diff: object = None
     _sell: dict = None
     _tiles: dict = None
+    _direct: object = None   # banded Cholesky factor (direct.BandCholesky), built on first direct solve
+
+    def direct_factor(self, coords=None):
+        """The banded Cholesky factor of K_ff (direct.BandCholesky; coords: the mesh's node
+        coordinates, for the ordering along the longest axis), cached."""
+        if self._direct is None:
+            from .direct import BandCholesky
+            self._direct = BandCholesky(self, coords=coords)
+        return self._direct
 
     def diff_operator(self):
         """The difference-form operator of the mixed block-PCG (7-byte values, 44-bit mantissas;

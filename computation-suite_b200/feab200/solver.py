@@ -441,8 +441,12 @@ class FESystem:
         t0 = time.perf_counter()
         op = self.reduced_operator(want32=(precision == "fp32"))
         Ff = self._reduced_rhs()
-        x, info = pcg_solve(op, Ff, x0=x0, tol=tol, maxiter=maxiter, precision=precision,
-                            use_dinv=(method != "cg"), reliable_delta=delta)
+        x = None
+        if method is None and precision == "fp64" and x0 is None:
+            x, info = self._direct_solve(op, Ff, tol, maxiter)
+        if x is None:
+            x, info = pcg_solve(op, Ff, x0=x0, tol=tol, maxiter=maxiter, precision=precision,
+                                use_dinv=(method != "cg"), reliable_delta=delta)
         self.last_solve_info = info
         if info.status == L.FEAB_NOT_SPD:
             raise np.linalg.LinAlgError("preconditioned_cg: p^T A p <= 0 -- A is not SPD.")
@@ -460,6 +464,67 @@ class FESystem:
                   f"relres={info.relres:.3e} reliable_updates={info.reliable_updates} "
                   f"time={time.perf_counter() - t0:.3f}s")
         return U
+
+    def _direct_solve(self, op, Ff, tol, maxiter):
+        """The sparse direct solve of method=None (_sparse_lu_solve, solver.py:1681-1724) as a
+        banded Cholesky on the GPU: (x, SolveInfo), or (None, None) when the band does not fit in
+        device memory (the Jacobi-PCG then takes over).
+
+        When the factor's pivots show a singular K_ff (min < 1e-10 max, the reference's test), the
+        reference solves densely by eigenvalues (_eigen_solve, solver.py:1584-1679) for the
+        minimum-norm least-squares answer pinv(K_ff) F.  Here the null space of K_ff is formed from
+        the mesh's rigid-body motions that vanish on the fixed DOFs; it is projected out of the
+        load, the consistent system is solved by Jacobi-PCG from x0 = 0, and it is projected out of
+        the result, which gives pinv(K_ff) F for a connected body."""
+        from .device import SolveInfo, pcg_solve, spmv
+        try:
+            fac = op.direct_factor(coords=self.mesh.nodes)
+        except MemoryError as e:
+            warnings.warn(f"solve_static: {e}; solving with Jacobi-PCG to tol {tol:g} instead.", UserWarning,
+                          stacklevel=4)
+            return None, None
+        except np.linalg.LinAlgError:
+            fac = None
+        b = torch.as_tensor(Ff, dtype=torch.float64).to(op.vals64.device)
+        if fac is None or fac.near_singular:
+            warnings.warn("solve_static: K_ff is singular to working precision (a pivot of its factorisation "
+                          "is below 1e-10 of the largest, e.g. a floating structure); returning the minimum-norm "
+                          "least-squares solution (rigid-body null space projected out, Jacobi-PCG on the rest).",
+                          UserWarning, stacklevel=4)
+            Z = self._rigid_null_space(op.vals64.device)
+            if Z is not None:
+                b = b - Z @ (Z.T @ b)
+            x, info = pcg_solve(op, b, tol=tol, maxiter=maxiter, precision="fp64")
+            if Z is not None:
+                x = x - Z @ (Z.T @ x)
+            return x, info
+        x = fac.solve(b)
+        bn = float(torch.linalg.norm(b)) or 1.0
+        rel = float(torch.linalg.norm(b - spmv(op, x, lanes_per_group=16))) / bn
+        return x, SolveInfo(L.FEAB_OK, 0, 0, rel, bn, "direct")
+
+    def _rigid_null_space(self, device):
+        """Orthonormal basis (n_free x k, k <= 6) of the rigid-body motions of the mesh (three
+        translations, three rotations about the centroid) that vanish on the fixed DOFs,
+        restricted to the free DOFs; None when no such motion exists."""
+        X = np.asarray(self.mesh.nodes, dtype=float)
+        c = X - X.mean(0)
+        R = np.zeros((3 * len(X), 6))
+        for k in range(3):
+            R[k::3, k] = 1.0
+        R[0::3, 3], R[1::3, 3] = -c[:, 1], c[:, 0]
+        R[1::3, 4], R[2::3, 4] = -c[:, 2], c[:, 1]
+        R[0::3, 5], R[2::3, 5] = c[:, 2], -c[:, 0]
+        fixed, free = self.fixed_dofs_array, self.free_dofs
+        N = np.eye(6)
+        if fixed.size:
+            _, sv, vt = np.linalg.svd(R[fixed], full_matrices=True)
+            rank = int(np.sum(sv > 1e-10 * max(sv.max(), 1e-300)))
+            N = vt[rank:].T
+        if N.shape[1] == 0:
+            return None
+        Q, _ = np.linalg.qr(R[free] @ N)
+        return torch.as_tensor(Q).to(device)
 
     def form_linear_system(self, F=None, K=None):
         from .linear_system import ReducedSystem

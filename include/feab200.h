@@ -529,6 +529,52 @@ int32_t feab_hex8_recover(const double* coords, const int32_t* conn, int64_t n_e
                           double* elem_vm, void* scratch, size_t scratch_bytes,
                           feab_device_status* status, cudaStream_t stream);
 
+/* ---------------------------------------------------------------- direct solve (banded Cholesky)
+ * Replaces the sparse direct solve of FESystem.solve_static() with method=None:
+ * FESystem._sparse_lu_solve (solver.py:1681-1724, SuperLU splu of K_ff, then a singularity test
+ * on the pivots: min |U_ii| < tol * max |U_ii|).  K_ff is SPD, so its LU without pivoting is
+ * its Cholesky factorisation and U_ii = L_ii^2; the same pivot test is reported.
+ *
+ * The rows are first renumbered (iperm: old row -> new row, a fill-reducing order such as
+ * reverse Cuthill-McKee) so that every nonzero lies within `bandwidth` of the diagonal.  The
+ * lower band is stored as 64 x 64 tiles: block row I (rows 64 I .. 64 I + 63) keeps the tiles of
+ * block columns I - bands .. I, tile (I, d) (block column I - d) at
+ * tiles + (I * (bands + 1) + d) * 4096, row major, where tiles = storage + 256 bytes (the first
+ * 256 bytes hold the factorisation's status and pivot range).  Rows past n are identity rows. */
+#define FEAB_BAND_TILE 64
+#define FEAB_BAND_HEADER_BYTES 256
+
+typedef struct feab_band {
+  int32_t n;          /* rows                                                  */
+  int32_t n_tiles;    /* block rows: ceil(n / 64)                              */
+  int32_t bands;      /* sub-diagonal tile columns kept: ceil(bandwidth / 64)  */
+  int32_t reserved;
+  void* storage;      /* feab_band_bytes(n, bandwidth) bytes of device memory, 256-byte aligned */
+} feab_band;
+
+/* The largest |iperm[i] - iperm[j]| over the nonzeros (i, j) of A.  scratch: 2 int32 of device
+ * memory.  An iperm entry outside [0, n) returns FEAB_BAD_ARG.  Synchronous. */
+int32_t feab_band_width(const feab_csr* A, const int32_t* iperm, int32_t* scratch, int32_t* bandwidth_out,
+                        cudaStream_t stream);
+
+/* Bytes of band storage (header + tiles) for n rows and the given bandwidth (0 if n <= 0). */
+size_t feab_band_bytes(int32_t n, int32_t bandwidth);
+
+/* Fills B with the lower band of the renumbered A; B->n, B->n_tiles and B->bands are set from
+ * n and bandwidth, B->storage must be set by the caller.  An entry outside the band returns
+ * FEAB_BAD_ARG.  Synchronous. */
+int32_t feab_band_assemble(const feab_csr* A, const int32_t* iperm, int32_t bandwidth, feab_band* B,
+                           cudaStream_t stream);
+
+/* In-place Cholesky factorisation B = L L^T (tile by tile, on the stream; synchronous).
+ * pivots_out[0] / [1]: the smallest and largest pivot L_ii^2 of rows < n.  A pivot <= 0 returns
+ * FEAB_NOT_SPD (the factor is then not usable). */
+int32_t feab_band_cholesky(feab_band* B, double* pivots_out, cudaStream_t stream);
+
+/* x = (L L^T)^{-1} b in the renumbered order (b, x and work: n_tiles * 64 doubles of device
+ * memory; the entries of b past n must be 0, and those of x past n are 0).  Asynchronous. */
+int32_t feab_band_solve(const feab_band* B, const double* b, double* x, double* work, cudaStream_t stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -189,7 +189,7 @@ def test_fesystem_drop_in_flow(golden):
     assert _rel(U, g["U_pcg"]) < 1e-11
     Um = fs.solve_static(method="pcg", tol=1e-10, precision="mixed")
     assert _rel(Um, g["U_lu"]) < UTOL
-    Ud = fs.solve_static()             # the reference's direct solve -> tight PCG here
+    Ud = fs.solve_static()             # the reference's direct solve: banded Cholesky here
     assert _rel(Ud, g["U_lu"]) < 1e-10
     rs = fs.form_linear_system()
     assert np.array_equal(rs.K.indptr, g["row_ptr"]) and np.array_equal(rs.K.indices, g["col_idx"])

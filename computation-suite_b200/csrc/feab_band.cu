@@ -11,11 +11,14 @@
 // Cholesky factor stays inside the band, so the factorisation is a right-looking tile algorithm
 // over block columns K = 0 .. n_tiles - 1:
 //   1. factor the diagonal tile (K, K) in shared memory (k_band_potrf);
-//   2. solve the tiles below it, L_IK = A_IK L_KK^{-T}, one CTA per tile (k_band_trsm);
+//      and invert its factor, Linv_KK = L_KK^{-1} (kept beside the band);
+//   2. form the tiles below it, L_IK = A_IK Linv_KK^T, one CTA per tile;
 //   3. update the trailing band, A_IJ -= L_IK L_JK^T for K < J <= I <= K + bands, one CTA per
-//      tile (k_band_update, a 64 x 64 x 64 FP64 product with 4 x 4 outputs per thread).
+//      tile (k_band_tile_gemm: 64 x 64 x 64 FP64 products with 4 x 4 outputs per thread).
+// Applying the inverted 64 x 64 diagonal factors (as blocked GPU triangular solvers do) turns the
+// per-column triangular solves into tile products, so only step 1 is sequential within a column.
 // The solves walk the block rows forward (L y = b) and backward (L^T x = y), one kernel per block
-// row: each CTA solves the block's 64 x 64 triangle with one warp and then applies one
+// row: each CTA forms the block's y_K = Linv_KK w_K (or x_K = Linv_KK^T w_K) and then applies one
 // off-diagonal tile to a later (earlier) block of the right-hand side.
 #include <algorithm>
 #include <cmath>
@@ -102,93 +105,139 @@ struct BandState {
 };
 static_assert(sizeof(BandState) <= FEAB_BAND_HEADER_BYTES, "band header");
 
-// Cholesky of the diagonal tile (K, K) in shared memory; pivots of rows < n are recorded.
-__global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, int bands, int K, int32_t n,
-                                                   BandState* st) {
-  __shared__ double A[kT][kLd];
-  __shared__ double dk;
+// Cholesky of the diagonal tile (K, K), then the inverse of its factor.  The tile lives in
+// registers, a 4 x 4 block per thread (16 x 16 threads); the right-looking elimination keeps the
+// columns unscaled (A_ij -= A_ik A_jk / p_k for j > k) and reads pivot column k from a shared
+// double buffer that its owners refill after each step, so one barrier separates the steps.  The
+// columns are scaled by 1 / sqrt(p_k) at the end.  Pivots of rows < n are recorded (a pivot <= 0
+// sets FEAB_NOT_SPD and is replaced by 1 so the kernel finishes).  Then Linv = L_KK^{-1} (lower
+// triangular, upper part 0) is formed column by column, 4 lanes per column, into inv.
+__global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, double* __restrict__ inv, int bands,
+                                                   int K, int32_t n, BandState* st) {
+  __shared__ double colbuf[2][kT];
+  __shared__ double piv[kT];
+  __shared__ double rd[kT];                 // 1 / L_ii
+  extern __shared__ __align__(16) double psm[];  // the factor and its inverse (dynamic: 66.5 KB)
+  double (*Ls)[kLd] = reinterpret_cast<double (*)[kLd]>(psm);
+  double (*Xs)[kLd] = reinterpret_cast<double (*)[kLd]>(psm + kT * kLd);
+  const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   double* T = tiles + tile_index(K, 0, bands);
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) A[q / kT][q % kT] = T[q];
-  __syncthreads();
+  double a[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const double2 p0 = *reinterpret_cast<const double2*>(T + (4 * ty + u) * kT + 4 * tx);
+    const double2 p1 = *reinterpret_cast<const double2*>(T + (4 * ty + u) * kT + 4 * tx + 2);
+    a[u][0] = p0.x;
+    a[u][1] = p0.y;
+    a[u][2] = p1.x;
+    a[u][3] = p1.y;
+  }
+  if (tx == 0) {
+#pragma unroll
+    for (int u = 0; u < 4; ++u) colbuf[0][4 * ty + u] = a[u][0];
+  }
   for (int k = 0; k < kT; ++k) {
-    if (threadIdx.x == 0) {
-      double p = A[k][k];
+    __syncthreads();
+    const double* col = colbuf[k & 1];
+    double p = col[k];
+    if (!(p > 0.0)) p = 1.0;
+    if (tid == 0) {
+      const double p0 = col[k];
       if (K * kT + k < n) {
-        if (p > 0.0) {
-          const unsigned long long b = (unsigned long long)__double_as_longlong(p);
+        if (p0 > 0.0) {
+          const unsigned long long b = (unsigned long long)__double_as_longlong(p0);
           atomicMin(&st->piv_min, b);
           atomicMax(&st->piv_max, b);
         } else {
           atomicCAS(&st->status, FEAB_OK, FEAB_NOT_SPD);
         }
       }
-      if (!(p > 0.0)) p = 1.0;  // keep going with a harmless pivot; the status reports it
-      dk = sqrt(p);
-      A[k][k] = dk;
+      piv[k] = p;
     }
-    __syncthreads();
-    for (int i = k + 1 + threadIdx.x; i < kT; i += blockDim.x) A[i][k] /= dk;
-    __syncthreads();
-    const int m = kT - 1 - k;
-    for (int q = threadIdx.x; q < m * m; q += blockDim.x) {
-      const int i = k + 1 + q / m, j = k + 1 + q % m;
-      if (j <= i) A[i][j] -= A[i][k] * A[j][k];
+    const double rp = 1.0 / p;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = 4 * ty + u;
+      const double ci = col[i] * rp;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int jj = 4 * tx + v;
+        if (jj > k && i >= jj) a[u][v] -= ci * col[jj];
+      }
     }
-    __syncthreads();
-  }
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
-    const int i = q / kT, j = q % kT;
-    if (j <= i) T[q] = A[i][j];
-  }
-}
-
-// L_IK = A_IK L_KK^{-T} for the tiles I = K + 1 + blockIdx.x below the diagonal: each row r of
-// the tile is a forward substitution x_c = (a_c - sum_{k<c} x_k L_ck) / L_cc, by 4 lanes that
-// split the sum (k = q mod 4) and combine it with two shuffles.
-__global__ void __launch_bounds__(256) k_band_trsm(double* __restrict__ tiles, int bands, int K) {
-  extern __shared__ __align__(16) double tsm[];  // two staged tiles (dynamic: 66.5 KB)
-  double (*L)[kLd] = reinterpret_cast<double (*)[kLd]>(tsm);
-  double (*X)[kLd] = reinterpret_cast<double (*)[kLd]>(tsm + kT * kLd);
-  const int I = K + 1 + blockIdx.x;
-  const double* Ld = tiles + tile_index(K, 0, bands);
-  double* T = tiles + tile_index(I, I - K, bands);
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
-    L[q / kT][q % kT] = Ld[q];
-    X[q / kT][q % kT] = T[q];
+    if (k + 1 < kT && tx == ((k + 1) >> 2)) {
+      const int cv = (k + 1) & 3;  // selected without indexing the register array at run time
+#pragma unroll
+      for (int u = 0; u < 4; ++u)
+        colbuf[(k + 1) & 1][4 * ty + u] = cv == 0 ? a[u][0] : cv == 1 ? a[u][1] : cv == 2 ? a[u][2] : a[u][3];
+    }
   }
   __syncthreads();
-  const int r = threadIdx.x >> 2, part = threadIdx.x & 3;
-  for (int c = 0; c < kT; ++c) {
-    double s = 0.0;
-    for (int k = part; k < c; k += 4) s += X[r][k] * L[c][k];
-    s += __shfl_xor_sync(FEAB_FULL_MASK, s, 1);
-    s += __shfl_xor_sync(FEAB_FULL_MASK, s, 2);
-    const double x = (X[r][c] - s) / L[c][c];
+  if (tid < kT) rd[tid] = 1.0 / sqrt(piv[tid]);
+  __syncthreads();
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int i = 4 * ty + u;
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int jj = 4 * tx + v;
+      const double l = i > jj ? a[u][v] * rd[jj] : (i == jj ? sqrt(piv[jj]) : 0.0);
+      Ls[i][jj] = l;
+      a[u][v] = l;
+    }
+    // the whole tile is written, with zeros above the diagonal
+    *reinterpret_cast<double2*>(T + i * kT + 4 * tx) = make_double2(a[u][0], a[u][1]);
+    *reinterpret_cast<double2*>(T + i * kT + 4 * tx + 2) = make_double2(a[u][2], a[u][3]);
+  }
+  __syncthreads();
+  // Linv column j: x_i = (delta_ij - sum_{j<=m<i} L_im x_m) / L_ii, rows ascending
+  const int jc = tid >> 2, part = tid & 3;
+  for (int i = 0; i < kT; ++i) {
+    double sum = 0.0;
+    for (int m = jc + part; m < i; m += 4) sum += Ls[i][m] * Xs[m][jc];
+    sum += __shfl_xor_sync(FEAB_FULL_MASK, sum, 1);
+    sum += __shfl_xor_sync(FEAB_FULL_MASK, sum, 2);
+    const double x = i < jc ? 0.0 : ((i == jc ? 1.0 : 0.0) - sum) * rd[i];
     __syncwarp();
-    if (part == 0) X[r][c] = x;
+    if (part == 0) Xs[i][jc] = x;
     __syncwarp();
   }
   __syncthreads();
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) T[q] = X[q / kT][q % kT];
+  double* Iv = inv + (size_t)K * kTile;
+  for (int q = tid; q < kTile; q += blockDim.x) Iv[q] = Xs[q / kT][q % kT];
 }
 
-// Trailing update of block column K: CTA a takes the pair (I, J) with K < J <= I, a = (I - K - 1)
-// (I - K) / 2 + (J - K - 1): A_IJ -= L_IK L_JK^T.  Each thread owns a 4 x 4 block of the tile;
-// the two factors are staged transposed (column k contiguous) so a thread reads its 4 rows and 4
+// C (op)= A B^T for 64 x 64 tiles, one CTA per output tile, 4 x 4 outputs per thread; the two
+// factors are staged transposed (column k contiguous) so that a thread reads its 4 rows and 4
 // columns of step k as two 16-byte loads each.
-__global__ void __launch_bounds__(256) k_band_update(double* __restrict__ tiles, int bands, int K) {
+//   UPDATE: the trailing update of block column K, CTA a -> (I, J) with K < J <= I, a = (I - K - 1)
+//           (I - K) / 2 + (J - K - 1): A_IJ -= L_IK L_JK^T;
+//   PANEL:  the panel below the diagonal tile, CTA b -> I = K + 1 + b: L_IK = A_IK Linv_KK^T.
+template <bool PANEL>
+__global__ void __launch_bounds__(256) k_band_tile_gemm(double* __restrict__ tiles, const double* __restrict__ inv,
+                                                       int bands, int K) {
   extern __shared__ __align__(16) double gsm[];
-  double* As = gsm;                  // As[k * kGemmLd + r] = L_IK[r][k]
-  double* Bs = gsm + kT * kGemmLd;   // Bs[k * kGemmLd + c] = L_JK[c][k]
-  const int a = blockIdx.x;
-  int io = (int)((sqrt(8.0 * a + 1.0) - 1.0) * 0.5);
-  while ((io + 1) * (io + 2) / 2 <= a) ++io;
-  while (io * (io + 1) / 2 > a) --io;
-  const int jo = a - io * (io + 1) / 2;
-  const int I = K + 1 + io, J = K + 1 + jo;
-  const double* Ap = tiles + tile_index(I, I - K, bands);
-  const double* Bp = tiles + tile_index(J, J - K, bands);
-  double* Cp = tiles + tile_index(I, I - J, bands);
+  double* As = gsm;                  // As[k * kGemmLd + r] = A[r][k]
+  double* Bs = gsm + kT * kGemmLd;   // Bs[k * kGemmLd + c] = B[c][k]
+  const double* Ap;
+  const double* Bp;
+  double* Cp;
+  if (PANEL) {
+    const int I = K + 1 + blockIdx.x;
+    Ap = tiles + tile_index(I, I - K, bands);
+    Bp = inv + (size_t)K * kTile;
+    Cp = tiles + tile_index(I, I - K, bands);
+  } else {
+    const int a = blockIdx.x;
+    int io = (int)((sqrt(8.0 * a + 1.0) - 1.0) * 0.5);
+    while ((io + 1) * (io + 2) / 2 <= a) ++io;
+    while (io * (io + 1) / 2 > a) --io;
+    const int jo = a - io * (io + 1) / 2;
+    const int I = K + 1 + io, J = K + 1 + jo;
+    Ap = tiles + tile_index(I, I - K, bands);
+    Bp = tiles + tile_index(J, J - K, bands);
+    Cp = tiles + tile_index(I, I - J, bands);
+  }
   for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
     const int row = q / kT, k = q % kT;
     As[k * kGemmLd + row] = Ap[q];
@@ -217,100 +266,80 @@ __global__ void __launch_bounds__(256) k_band_update(double* __restrict__ tiles,
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
     double2* c = reinterpret_cast<double2*>(Cp + (size_t)(4 * tr + u) * kT + 4 * tc);
-    double2 c01 = c[0], c23 = c[1];
-    c01.x -= acc[u][0];
-    c01.y -= acc[u][1];
-    c23.x -= acc[u][2];
-    c23.y -= acc[u][3];
-    c[0] = c01;
-    c[1] = c23;
+    if (PANEL) {
+      c[0] = make_double2(acc[u][0], acc[u][1]);
+      c[1] = make_double2(acc[u][2], acc[u][3]);
+    } else {
+      double2 c01 = c[0], c23 = c[1];
+      c01.x -= acc[u][0];
+      c01.y -= acc[u][1];
+      c23.x -= acc[u][2];
+      c23.y -= acc[u][3];
+      c[0] = c01;
+      c[1] = c23;
+    }
   }
 }
-constexpr size_t kUpdateSmem = 2 * kT * kGemmLd * sizeof(double);
-constexpr size_t kTrsmSmem = 2 * kT * kLd * sizeof(double);
+constexpr size_t kGemmSmem = 2 * kT * kGemmLd * sizeof(double);
+constexpr size_t kPotrfSmem = 2 * kT * kLd * sizeof(double);
 
 // ---------------------------------------------------------------- solves
-// Forward step K of L y = b: every CTA solves L_KK y_K = w_K with warp 0 (lane l owns rows l and
-// l + 32; column c's value is broadcast by shuffle), CTA 0 writes y_K, and CTA i < n_below applies
-// tile (K + 1 + i, i + 1): w_{K+1+i} -= L_{K+1+i,K} y_K (two threads per row).
-__global__ void __launch_bounds__(128) k_band_fwd(const double* __restrict__ tiles, int bands, int K, int n_below,
-                                                 double* __restrict__ w, double* __restrict__ y) {
-  __shared__ double L[kT][kLd];
+// Forward step K of L y = b: every CTA forms y_K = Linv_KK w_K (two threads per row), CTA 0 writes
+// it, and CTA i < n_below applies tile (K + 1 + i, i + 1): w_{K+1+i} -= L_{K+1+i,K} y_K.
+__global__ void __launch_bounds__(128) k_band_fwd(const double* __restrict__ tiles, const double* __restrict__ inv,
+                                                 int bands, int K, int n_below, double* __restrict__ w,
+                                                 double* __restrict__ y) {
+  __shared__ double wk[kT];
   __shared__ double ys[kT];
-  const double* Ld = tiles + tile_index(K, 0, bands);
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) L[q / kT][q % kT] = Ld[q];
+  if (threadIdx.x < kT) wk[threadIdx.x] = w[K * kT + threadIdx.x];
   __syncthreads();
-  if (threadIdx.x < 32) {
-    const int l = threadIdx.x;
-    double v0 = w[K * kT + l], v1 = w[K * kT + l + 32];
-    for (int c = 0; c < kT; ++c) {
-      const int owner = c & 31;
-      double t = 0.0;
-      if (l == owner) t = (c < 32 ? v0 : v1) / L[c][c];
-      const double yc = __shfl_sync(FEAB_FULL_MASK, t, owner);
-      if (l == owner) {
-        if (c < 32) v0 = yc;
-        else v1 = yc;
-      }
-      if (l > c) v0 -= L[l][c] * yc;
-      if (l + 32 > c) v1 -= L[l + 32][c] * yc;
-    }
-    ys[l] = v0;
-    ys[l + 32] = v1;
-  }
+  const int r = threadIdx.x >> 1, h = threadIdx.x & 1;
+  const double* Iv = inv + (size_t)K * kTile;
+  double s = 0.0;
+#pragma unroll 8
+  for (int c = 32 * h; c < 32 * h + 32; ++c) s += Iv[r * kT + c] * wk[c];
+  s += __shfl_xor_sync(FEAB_FULL_MASK, s, 1);
+  if (h == 0) ys[r] = s;
   __syncthreads();
   if (blockIdx.x == 0 && threadIdx.x < kT) y[K * kT + threadIdx.x] = ys[threadIdx.x];
   if ((int)blockIdx.x < n_below) {
     const int I = K + 1 + blockIdx.x;
     const double* T = tiles + tile_index(I, I - K, bands);
-    const int r = threadIdx.x >> 1, h = threadIdx.x & 1;
-    double s = 0.0;
+    double t = 0.0;
 #pragma unroll 8
-    for (int c = 32 * h; c < 32 * h + 32; ++c) s += T[(size_t)r * kT + c] * ys[c];
-    s += __shfl_xor_sync(FEAB_FULL_MASK, s, 1);
-    if (h == 0) w[I * kT + r] -= s;
+    for (int c = 32 * h; c < 32 * h + 32; ++c) t += T[(size_t)r * kT + c] * ys[c];
+    t += __shfl_xor_sync(FEAB_FULL_MASK, t, 1);
+    if (h == 0) w[I * kT + r] -= t;
   }
 }
 
-// Backward step K of L^T x = y: every CTA solves L_KK^T x_K = w_K (rows descending), CTA 0 writes
-// x_K, and CTA i < n_above applies tile (K, i + 1) transposed: w_{K-1-i} -= L_{K,K-1-i}^T x_K (two
-// threads per column, each summing half of the rows).
-__global__ void __launch_bounds__(128) k_band_bwd(const double* __restrict__ tiles, int bands, int K, int n_above,
-                                                 double* __restrict__ w, double* __restrict__ x) {
-  __shared__ double L[kT][kLd];
+// Backward step K of L^T x = y: every CTA forms x_K = Linv_KK^T w_K (two threads per column), CTA
+// 0 writes it, and CTA i < n_above applies tile (K, i + 1) transposed: w_{K-1-i} -= L_{K,K-1-i}^T
+// x_K.
+__global__ void __launch_bounds__(128) k_band_bwd(const double* __restrict__ tiles, const double* __restrict__ inv,
+                                                 int bands, int K, int n_above, double* __restrict__ w,
+                                                 double* __restrict__ x) {
+  __shared__ double wk[kT];
   __shared__ double xs[kT];
-  const double* Ld = tiles + tile_index(K, 0, bands);
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) L[q / kT][q % kT] = Ld[q];
+  if (threadIdx.x < kT) wk[threadIdx.x] = w[K * kT + threadIdx.x];
   __syncthreads();
-  if (threadIdx.x < 32) {
-    const int l = threadIdx.x;
-    double v0 = w[K * kT + l], v1 = w[K * kT + l + 32];
-    for (int r = kT - 1; r >= 0; --r) {
-      const int owner = r & 31;
-      double t = 0.0;
-      if (l == owner) t = (r < 32 ? v0 : v1) / L[r][r];
-      const double xr = __shfl_sync(FEAB_FULL_MASK, t, owner);
-      if (l == owner) {
-        if (r < 32) v0 = xr;
-        else v1 = xr;
-      }
-      if (l < r) v0 -= L[r][l] * xr;
-      if (l + 32 < r) v1 -= L[r][l + 32] * xr;
-    }
-    xs[l] = v0;
-    xs[l + 32] = v1;
-  }
+  const int c = threadIdx.x >> 1, h = threadIdx.x & 1;
+  const double* Iv = inv + (size_t)K * kTile;
+  double s = 0.0;
+#pragma unroll 8
+  for (int r = 32 * h; r < 32 * h + 32; ++r) s += Iv[r * kT + c] * wk[r];
+  s += __shfl_xor_sync(FEAB_FULL_MASK, s, 1);
+  if (h == 0) xs[c] = s;
   __syncthreads();
   if (blockIdx.x == 0 && threadIdx.x < kT) x[K * kT + threadIdx.x] = xs[threadIdx.x];
   if ((int)blockIdx.x < n_above) {
     const int J = K - 1 - blockIdx.x;
     const double* T = tiles + tile_index(K, K - J, bands);
-    const int c = threadIdx.x >> 1, h = threadIdx.x & 1;
-    double s = 0.0;
+    double t = 0.0;
 #pragma unroll 8
-    for (int r = 32 * h; r < 32 * h + 32; ++r) s += T[(size_t)r * kT + c] * xs[r];
-    s += __shfl_xor_sync(FEAB_FULL_MASK, s, 1);
-    if (h == 0) w[J * kT + c] -= s;
+    for (int r = 32 * h; r < 32 * h + 32; ++r) t += T[(size_t)r * kT + c] * xs[r];
+    t += __shfl_xor_sync(FEAB_FULL_MASK, t, 1);
+    if (h == 0) w[J * kT + c] -= t;
   }
 }
 
@@ -325,6 +354,10 @@ BandState* band_state(const feab_band* B) { return reinterpret_cast<BandState*>(
 double* band_tiles(const feab_band* B) {
   return reinterpret_cast<double*>(static_cast<char*>(B->storage) + FEAB_BAND_HEADER_BYTES);
 }
+// The inverses of the diagonal factor tiles, one per block row, after the band.
+double* band_inv(const feab_band* B) {
+  return band_tiles(B) + (size_t)B->n_tiles * (size_t)(B->bands + 1) * kTile;
+}
 bool band_ok(const feab_band* B) {
   return B && B->storage && B->n > 0 && B->bands >= 0 && B->n_tiles == (B->n + kT - 1) / kT &&
          (reinterpret_cast<uintptr_t>(B->storage) & 255) == 0;
@@ -334,7 +367,7 @@ bool band_ok(const feab_band* B) {
 extern "C" size_t feab_band_bytes(int32_t n, int32_t bandwidth) {
   if (n <= 0 || bandwidth < 0) return 0;
   const size_t nt = (size_t)(n + kT - 1) / kT, bands = (size_t)(bandwidth + kT - 1) / kT;
-  return FEAB_BAND_HEADER_BYTES + nt * (bands + 1) * (size_t)kTile * sizeof(double);
+  return FEAB_BAND_HEADER_BYTES + nt * (bands + 2) * (size_t)kTile * sizeof(double);
 }
 
 extern "C" int32_t feab_band_width(const feab_csr* A, const int32_t* iperm, int32_t* scratch, int32_t* bandwidth_out,
@@ -382,17 +415,21 @@ extern "C" int32_t feab_band_cholesky(feab_band* B, double* pivots_out, cudaStre
   init.piv_max = 0ull;
   BandState* st = band_state(B);
   FEAB_CUDA(cudaMemcpyAsync(st, &init, sizeof(BandState), cudaMemcpyHostToDevice, s));
-  FEAB_CUDA(cudaFuncSetAttribute(k_band_update, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kUpdateSmem));
-  FEAB_CUDA(cudaFuncSetAttribute(k_band_trsm, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kTrsmSmem));
+  FEAB_CUDA(cudaFuncSetAttribute(k_band_potrf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPotrfSmem));
+  FEAB_CUDA(cudaFuncSetAttribute(k_band_tile_gemm<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kGemmSmem));
+  FEAB_CUDA(cudaFuncSetAttribute(k_band_tile_gemm<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)kGemmSmem));
   double* tiles = band_tiles(B);
+  double* inv = band_inv(B);
   const int NT = B->n_tiles, bands = B->bands;
   uint64_t launches = 0;
   for (int K = 0; K < NT; ++K) {
-    k_band_potrf<<<1, 256, 0, s>>>(tiles, bands, K, B->n, st);
+    k_band_potrf<<<1, 256, kPotrfSmem, s>>>(tiles, inv, bands, K, B->n, st);
     const int below = std::min(bands, NT - 1 - K);
     if (below > 0) {
-      k_band_trsm<<<below, 256, kTrsmSmem, s>>>(tiles, bands, K);
-      k_band_update<<<below * (below + 1) / 2, 256, kUpdateSmem, s>>>(tiles, bands, K);
+      k_band_tile_gemm<true><<<below, 256, kGemmSmem, s>>>(tiles, inv, bands, K);
+      k_band_tile_gemm<false><<<below * (below + 1) / 2, 256, kGemmSmem, s>>>(tiles, inv, bands, K);
       launches += 2;
     }
     launches += 1;
@@ -415,18 +452,19 @@ extern "C" int32_t feab_band_cholesky(feab_band* B, double* pivots_out, cudaStre
 extern "C" int32_t feab_band_solve(const feab_band* B, const double* b, double* x, double* work, cudaStream_t s) {
   if (!band_ok(B) || !b || !x || !work || x == b || x == work || b == work) return FEAB_BAD_ARG;
   const double* tiles = band_tiles(B);
+  const double* inv = band_inv(B);
   const int NT = B->n_tiles, bands = B->bands;
   const size_t bytes = (size_t)NT * kT * sizeof(double);
   // forward: work = b, updated in place; y into x
   FEAB_CUDA(cudaMemcpyAsync(work, b, bytes, cudaMemcpyDeviceToDevice, s));
   for (int K = 0; K < NT; ++K) {
     const int below = std::min(bands, NT - 1 - K);
-    k_band_fwd<<<std::max(1, below), 128, 0, s>>>(tiles, bands, K, below, work, x);
+    k_band_fwd<<<std::max(1, below), 128, 0, s>>>(tiles, inv, bands, K, below, work, x);
   }
   // backward: x (= y) updated in place; the solution into work, then copied to x
   for (int K = NT - 1; K >= 0; --K) {
     const int above = std::min(bands, K);
-    k_band_bwd<<<std::max(1, above), 128, 0, s>>>(tiles, bands, K, above, x, work);
+    k_band_bwd<<<std::max(1, above), 128, 0, s>>>(tiles, inv, bands, K, above, x, work);
   }
   count_launches(2 * (uint64_t)NT);
   FEAB_CHECK_LAUNCH();

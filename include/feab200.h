@@ -540,7 +540,8 @@ int32_t feab_hex8_recover(const double* coords, const int32_t* conn, int64_t n_e
  * lower band is stored as 64 x 64 tiles: block row I (rows 64 I .. 64 I + 63) keeps the tiles of
  * block columns I - bands .. I, tile (I, d) (block column I - d) at
  * tiles + (I * (bands + 1) + d) * 4096, row major, where tiles = storage + 256 bytes (the first
- * 256 bytes hold the factorisation's status and pivot range).  Rows past n are identity rows. */
+ * 256 bytes hold the factorisation's status and pivot range).  After the band, n_tiles more tiles
+ * hold the inverses of the diagonal factor tiles.  Rows past n are identity rows. */
 #define FEAB_BAND_TILE 64
 #define FEAB_BAND_HEADER_BYTES 256
 
@@ -557,7 +558,8 @@ typedef struct feab_band {
 int32_t feab_band_width(const feab_csr* A, const int32_t* iperm, int32_t* scratch, int32_t* bandwidth_out,
                         cudaStream_t stream);
 
-/* Bytes of band storage (header + tiles) for n rows and the given bandwidth (0 if n <= 0). */
+/* Bytes of band storage (header, band tiles, inverse diagonal tiles) for n rows and the given
+ * bandwidth (0 if n <= 0). */
 size_t feab_band_bytes(int32_t n, int32_t bandwidth);
 
 /* Fills B with the lower band of the renumbered A; B->n, B->n_tiles and B->bands are set from

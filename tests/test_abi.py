@@ -41,9 +41,10 @@ def test_workspace_queries_do_not_need_a_gpu():
     assert _lib.lib.feab_pcg_workspace_bytes(1000, _lib.PREC_MIXED) >= 3 * 8 * 1000 + 4 * 4 * 1000
     assert _lib.lib.feab_pcg_workspace_bytes(10, 7) == 0
     assert _lib.lib.feab_topology_scratch_bytes(100, 50) > 0
-    # banded Cholesky: 256-byte header + n_tiles * (bands + 1) tiles of 64 x 64 doubles
-    assert _lib.lib.feab_band_bytes(100, 130) == 256 + 2 * 4 * 64 * 64 * 8
-    assert _lib.lib.feab_band_bytes(64, 0) == 256 + 64 * 64 * 8
+    # banded Cholesky: 256-byte header + n_tiles * (bands + 1) band tiles + n_tiles inverse
+    # diagonal tiles, each 64 x 64 doubles
+    assert _lib.lib.feab_band_bytes(100, 130) == 256 + 2 * 5 * 64 * 64 * 8
+    assert _lib.lib.feab_band_bytes(64, 0) == 256 + 2 * 64 * 64 * 8
     assert _lib.lib.feab_band_bytes(0, 10) == 0
 
 

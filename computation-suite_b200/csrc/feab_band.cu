@@ -14,7 +14,7 @@
 //      and invert its factor, Linv_KK = L_KK^{-1} (kept beside the band);
 //   2. form the tiles below it, L_IK = A_IK Linv_KK^T, one CTA per tile;
 //   3. update the trailing band, A_IJ -= L_IK L_JK^T for K < J <= I <= K + bands, one CTA per
-//      tile (k_band_tile_gemm: 64 x 64 x 64 FP64 products with 4 x 4 outputs per thread).
+//      tile (k_band_tile_gemm: 64 x 64 x 64 FP64 products on the FP64 tensor path, mma.sync).
 // Applying the inverted 64 x 64 diagonal factors (as blocked GPU triangular solvers do) turns the
 // per-column triangular solves into tile products, so only step 1 is sequential within a column.
 // The solves walk the block rows forward (L y = b) and backward (L^T x = y), one kernel per block
@@ -31,7 +31,6 @@ namespace {
 constexpr int kT = FEAB_BAND_TILE;       // tile edge
 constexpr int kTile = kT * kT;           // doubles per tile
 constexpr int kLd = kT + 1;              // shared-memory row stride of a staged triangle
-constexpr int kGemmLd = kT + 2;          // row stride of the update's staged operands (16-byte rows)
 
 __host__ __device__ inline size_t tile_index(int I, int d, int bands) {
   return ((size_t)I * (size_t)(bands + 1) + (size_t)d) * (size_t)kTile;
@@ -106,20 +105,21 @@ struct BandState {
 static_assert(sizeof(BandState) <= FEAB_BAND_HEADER_BYTES, "band header");
 
 // Cholesky of the diagonal tile (K, K), then the inverse of its factor.  The tile lives in
-// registers, a 4 x 4 block per thread (16 x 16 threads); the right-looking elimination keeps the
-// columns unscaled (A_ij -= A_ik A_jk / p_k for j > k) and reads pivot column k from a shared
-// double buffer that its owners refill after each step, so one barrier separates the steps.  The
-// columns are scaled by 1 / sqrt(p_k) at the end.  Pivots of rows < n are recorded (a pivot <= 0
-// sets FEAB_NOT_SPD and is replaced by 1 so the kernel finishes).  Then Linv = L_KK^{-1} (lower
-// triangular, upper part 0) is formed column by column, 4 lanes per column, into inv.
+// registers, a 4 x 4 block per thread (16 x 16 threads).  The right-looking elimination keeps the
+// columns unscaled (A_ij -= A_ik A_jk / p_k for j > k): the owners of column k + 1 copy it into a
+// shared double buffer after their step-k update, and the owner of its diagonal entry stores
+// 1 / p_{k+1}, so one barrier separates the steps.  The columns are scaled by 1 / sqrt(p_k) at the
+// end.  Pivots of rows < n are recorded (a pivot <= 0 sets FEAB_NOT_SPD and is replaced by 1 so the
+// kernel finishes).  Linv = L_KK^{-1} (lower triangular) is then formed the same way: X = I in
+// registers, and for each row m, X_m = X_m / L_mm is published and X_i -= L_im X_m for i > m.
 __global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, double* __restrict__ inv, int bands,
                                                    int K, int32_t n, BandState* st) {
   __shared__ double colbuf[2][kT];
+  __shared__ double rpbuf[2];
   __shared__ double piv[kT];
-  __shared__ double rd[kT];                 // 1 / L_ii
-  extern __shared__ __align__(16) double psm[];  // the factor and its inverse (dynamic: 66.5 KB)
+  __shared__ double rowbuf[2][kT];
+  extern __shared__ __align__(16) double psm[];  // the factor L (dynamic: 33 KB)
   double (*Ls)[kLd] = reinterpret_cast<double (*)[kLd]>(psm);
-  double (*Xs)[kLd] = reinterpret_cast<double (*)[kLd]>(psm + kT * kLd);
   const int tid = threadIdx.x, ty = tid >> 4, tx = tid & 15;
   double* T = tiles + tile_index(K, 0, bands);
   double a[4][4];
@@ -132,29 +132,39 @@ __global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, 
     a[u][2] = p1.x;
     a[u][3] = p1.y;
   }
+  // a[u][v] for run-time u, v, selected without indexing the register array
+  auto row = [&](int u, int v) {
+    return v == 0 ? a[u][0] : v == 1 ? a[u][1] : v == 2 ? a[u][2] : a[u][3];
+  };
+  auto sel = [&](int u, int v) {
+    return u == 0 ? row(0, v) : u == 1 ? row(1, v) : u == 2 ? row(2, v) : row(3, v);
+  };
   if (tx == 0) {
 #pragma unroll
     for (int u = 0; u < 4; ++u) colbuf[0][4 * ty + u] = a[u][0];
+    if (ty == 0) {
+      const double p = a[0][0] > 0.0 ? a[0][0] : 1.0;
+      rpbuf[0] = 1.0 / p;
+    }
   }
+  double pmin = INFINITY, pmax = 0.0;
+  bool bad = false;
   for (int k = 0; k < kT; ++k) {
     __syncthreads();
     const double* col = colbuf[k & 1];
-    double p = col[k];
-    if (!(p > 0.0)) p = 1.0;
+    const double rp = rpbuf[k & 1];
     if (tid == 0) {
       const double p0 = col[k];
       if (K * kT + k < n) {
         if (p0 > 0.0) {
-          const unsigned long long b = (unsigned long long)__double_as_longlong(p0);
-          atomicMin(&st->piv_min, b);
-          atomicMax(&st->piv_max, b);
+          pmin = fmin(pmin, p0);
+          pmax = fmax(pmax, p0);
         } else {
-          atomicCAS(&st->status, FEAB_OK, FEAB_NOT_SPD);
+          bad = true;
         }
       }
-      piv[k] = p;
+      piv[k] = p0 > 0.0 ? p0 : 1.0;
     }
-    const double rp = 1.0 / p;
 #pragma unroll
     for (int u = 0; u < 4; ++u) {
       const int i = 4 * ty + u;
@@ -165,15 +175,23 @@ __global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, 
         if (jj > k && i >= jj) a[u][v] -= ci * col[jj];
       }
     }
-    if (k + 1 < kT && tx == ((k + 1) >> 2)) {
-      const int cv = (k + 1) & 3;  // selected without indexing the register array at run time
+    const int k1 = k + 1;
+    if (k1 < kT && tx == (k1 >> 2)) {
 #pragma unroll
-      for (int u = 0; u < 4; ++u)
-        colbuf[(k + 1) & 1][4 * ty + u] = cv == 0 ? a[u][0] : cv == 1 ? a[u][1] : cv == 2 ? a[u][2] : a[u][3];
+      for (int u = 0; u < 4; ++u) colbuf[k1 & 1][4 * ty + u] = sel(u, k1 & 3);
+      if (ty == (k1 >> 2)) {
+        const double p = sel(k1 & 3, k1 & 3);
+        rpbuf[k1 & 1] = 1.0 / (p > 0.0 ? p : 1.0);
+      }
     }
   }
-  __syncthreads();
-  if (tid < kT) rd[tid] = 1.0 / sqrt(piv[tid]);
+  if (tid == 0) {
+    if (pmax > 0.0) {
+      atomicMin(&st->piv_min, (unsigned long long)__double_as_longlong(pmin));
+      atomicMax(&st->piv_max, (unsigned long long)__double_as_longlong(pmax));
+    }
+    if (bad) atomicCAS(&st->status, FEAB_OK, FEAB_NOT_SPD);
+  }
   __syncthreads();
 #pragma unroll
   for (int u = 0; u < 4; ++u) {
@@ -181,7 +199,7 @@ __global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, 
 #pragma unroll
     for (int v = 0; v < 4; ++v) {
       const int jj = 4 * tx + v;
-      const double l = i > jj ? a[u][v] * rd[jj] : (i == jj ? sqrt(piv[jj]) : 0.0);
+      const double l = i > jj ? a[u][v] * rsqrt(piv[jj]) : (i == jj ? sqrt(piv[jj]) : 0.0);
       Ls[i][jj] = l;
       a[u][v] = l;
     }
@@ -189,36 +207,72 @@ __global__ void __launch_bounds__(256) k_band_potrf(double* __restrict__ tiles, 
     *reinterpret_cast<double2*>(T + i * kT + 4 * tx) = make_double2(a[u][0], a[u][1]);
     *reinterpret_cast<double2*>(T + i * kT + 4 * tx + 2) = make_double2(a[u][2], a[u][3]);
   }
+  // Linv: X = I; row m final after dividing by L_mm; rows below take X_i -= L_im X_m
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) a[u][v] = (4 * ty + u == 4 * tx + v) ? 1.0 : 0.0;
   __syncthreads();
-  // Linv column j: x_i = (delta_ij - sum_{j<=m<i} L_im x_m) / L_ii, rows ascending
-  const int jc = tid >> 2, part = tid & 3;
-  for (int i = 0; i < kT; ++i) {
-    double sum = 0.0;
-    for (int m = jc + part; m < i; m += 4) sum += Ls[i][m] * Xs[m][jc];
-    sum += __shfl_xor_sync(FEAB_FULL_MASK, sum, 1);
-    sum += __shfl_xor_sync(FEAB_FULL_MASK, sum, 2);
-    const double x = i < jc ? 0.0 : ((i == jc ? 1.0 : 0.0) - sum) * rd[i];
-    __syncwarp();
-    if (part == 0) Xs[i][jc] = x;
-    __syncwarp();
+  if (ty == 0) {
+    const double rl = 1.0 / Ls[0][0];
+#pragma unroll
+    for (int v = 0; v < 4; ++v) rowbuf[0][4 * tx + v] = a[0][v] * rl;
   }
-  __syncthreads();
+  for (int m = 0; m < kT; ++m) {
+    __syncthreads();
+    const double* xm = rowbuf[m & 1];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int i = 4 * ty + u;
+      if (i == m) {
+#pragma unroll
+        for (int v = 0; v < 4; ++v) a[u][v] = xm[4 * tx + v];
+      } else if (i > m) {
+        const double lim = Ls[i][m];
+#pragma unroll
+        for (int v = 0; v < 4; ++v) a[u][v] -= lim * xm[4 * tx + v];
+      }
+    }
+    const int m1 = m + 1;
+    if (m1 < kT && ty == (m1 >> 2)) {
+      const double rl = 1.0 / Ls[m1][m1];
+      const int u = m1 & 3;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) rowbuf[m1 & 1][4 * tx + v] = sel(u, v) * rl;
+    }
+  }
   double* Iv = inv + (size_t)K * kTile;
-  for (int q = tid; q < kTile; q += blockDim.x) Iv[q] = Xs[q / kT][q % kT];
+#pragma unroll
+  for (int u = 0; u < 4; ++u) {
+    const int i = 4 * ty + u;
+    *reinterpret_cast<double2*>(Iv + i * kT + 4 * tx) = make_double2(a[u][0], a[u][1]);
+    *reinterpret_cast<double2*>(Iv + i * kT + 4 * tx + 2) = make_double2(a[u][2], a[u][3]);
+  }
 }
 
-// C (op)= A B^T for 64 x 64 tiles, one CTA per output tile, 4 x 4 outputs per thread; the two
-// factors are staged transposed (column k contiguous) so that a thread reads its 4 rows and 4
-// columns of step k as two 16-byte loads each.
+// C (op)= A B^T for 64 x 64 tiles on the FP64 tensor path (mma.sync m8n8k4), one CTA per output
+// tile: warp w owns rows 8 w .. 8 w + 7 and all 64 columns (eight 8 x 8 accumulators), and walks k
+// in steps of 4.  Fragments (m8n8k4, .f64): A row-major 8 x 4, lane l holds (l / 4, l % 4); B
+// column-major 4 x 8, lane l holds (l % 4, l / 4); C 8 x 8, lane l holds (l / 4, 2 (l % 4) + i).
+// Both factors are staged row-major in shared memory with a padded row (kMmaLd doubles), so each
+// fragment load of a half-warp touches 16 distinct banks.
 //   UPDATE: the trailing update of block column K, CTA a -> (I, J) with K < J <= I, a = (I - K - 1)
 //           (I - K) / 2 + (J - K - 1): A_IJ -= L_IK L_JK^T;
 //   PANEL:  the panel below the diagonal tile, CTA b -> I = K + 1 + b: L_IK = A_IK Linv_KK^T.
+constexpr int kMmaLd = kT + 4;
+
+__device__ __forceinline__ void dmma884(double (&d)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+               : "+d"(d[0]), "+d"(d[1])
+               : "d"(a), "d"(b));
+}
+
 template <bool PANEL>
 __global__ void __launch_bounds__(256) k_band_tile_gemm(double* __restrict__ tiles, const double* __restrict__ inv,
                                                        int bands, int K) {
   extern __shared__ __align__(16) double gsm[];
-  double* As = gsm;                  // As[k * kGemmLd + r] = A[r][k]
-  double* Bs = gsm + kT * kGemmLd;   // Bs[k * kGemmLd + c] = B[c][k]
+  double* As = gsm;                  // As[r * kMmaLd + k] = A[r][k]
+  double* Bs = gsm + kT * kMmaLd;    // Bs[c * kMmaLd + k] = B[c][k]
   const double* Ap;
   const double* Bp;
   double* Cp;
@@ -238,50 +292,43 @@ __global__ void __launch_bounds__(256) k_band_tile_gemm(double* __restrict__ til
     Bp = tiles + tile_index(J, J - K, bands);
     Cp = tiles + tile_index(I, I - J, bands);
   }
-  for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
-    const int row = q / kT, k = q % kT;
-    As[k * kGemmLd + row] = Ap[q];
-    Bs[k * kGemmLd + row] = Bp[q];
+  for (int q = threadIdx.x; q < kTile / 2; q += blockDim.x) {
+    const int row = q / (kT / 2), k2 = q % (kT / 2);
+    *reinterpret_cast<double2*>(As + row * kMmaLd + 2 * k2) = reinterpret_cast<const double2*>(Ap)[q];
+    *reinterpret_cast<double2*>(Bs + row * kMmaLd + 2 * k2) = reinterpret_cast<const double2*>(Bp)[q];
   }
   __syncthreads();
-  const int tr = threadIdx.x >> 4, tc = threadIdx.x & 15;
-  double acc[4][4];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, t = lane & 3;
+  double acc[8][2];
 #pragma unroll
-  for (int u = 0; u < 4; ++u)
-#pragma unroll
-    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = 0.0;
+  const double* Arow = As + (8 * warp + g) * kMmaLd + t;
+  const double* Bcol = Bs + g * kMmaLd + t;
 #pragma unroll 4
-  for (int k = 0; k < kT; ++k) {
-    const double2 a01 = *reinterpret_cast<const double2*>(As + k * kGemmLd + 4 * tr);
-    const double2 a23 = *reinterpret_cast<const double2*>(As + k * kGemmLd + 4 * tr + 2);
-    const double2 b01 = *reinterpret_cast<const double2*>(Bs + k * kGemmLd + 4 * tc);
-    const double2 b23 = *reinterpret_cast<const double2*>(Bs + k * kGemmLd + 4 * tc + 2);
-    const double av[4] = {a01.x, a01.y, a23.x, a23.y};
-    const double bv[4] = {b01.x, b01.y, b23.x, b23.y};
+  for (int k0 = 0; k0 < kT; k0 += 4) {
+    const double a = Arow[k0];
+    double b[8];
 #pragma unroll
-    for (int u = 0; u < 4; ++u)
+    for (int j = 0; j < 8; ++j) b[j] = Bcol[8 * j * kMmaLd + k0];
 #pragma unroll
-      for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+    for (int j = 0; j < 8; ++j) dmma884(acc[j], a, b[j]);
   }
+  const int r = 8 * warp + g;
 #pragma unroll
-  for (int u = 0; u < 4; ++u) {
-    double2* c = reinterpret_cast<double2*>(Cp + (size_t)(4 * tr + u) * kT + 4 * tc);
+  for (int j = 0; j < 8; ++j) {
+    double2* c = reinterpret_cast<double2*>(Cp + (size_t)r * kT + 8 * j + 2 * t);
     if (PANEL) {
-      c[0] = make_double2(acc[u][0], acc[u][1]);
-      c[1] = make_double2(acc[u][2], acc[u][3]);
+      *c = make_double2(acc[j][0], acc[j][1]);
     } else {
-      double2 c01 = c[0], c23 = c[1];
-      c01.x -= acc[u][0];
-      c01.y -= acc[u][1];
-      c23.x -= acc[u][2];
-      c23.y -= acc[u][3];
-      c[0] = c01;
-      c[1] = c23;
+      double2 cv = *c;
+      cv.x -= acc[j][0];
+      cv.y -= acc[j][1];
+      *c = cv;
     }
   }
 }
-constexpr size_t kGemmSmem = 2 * kT * kGemmLd * sizeof(double);
-constexpr size_t kPotrfSmem = 2 * kT * kLd * sizeof(double);
+constexpr size_t kGemmSmem = 2 * kT * kMmaLd * sizeof(double);
+constexpr size_t kPotrfSmem = kT * kLd * sizeof(double);
 
 // ---------------------------------------------------------------- solves
 // Forward step K of L y = b: every CTA forms y_K = Linv_KK w_K (two threads per row), CTA 0 writes

@@ -9,8 +9,10 @@ vector F and the boundary-condition bookkeeping stay host-side numpy, as in the 
 
 Differences, by design:
 - Hex8Solid3D, single block, method="full" only (others raise NotImplementedError).
-- solve_static(method=None) (the reference's SuperLU direct solve) runs the FP64 Jacobi-PCG
-  to a relative residual of 1e-12 instead; there is no direct factorisation on this path.
+- solve_static(method=None) (the reference's SuperLU direct solve) factors K_ff with a banded
+  Cholesky on the GPU (feab200.direct) and reuses the factor for later loads; a band that does
+  not fit in device memory falls back to Jacobi-PCG to 1e-12, and a singular K_ff gives the
+  minimum-norm least-squares solution, as the reference's eigenvalue fallback does.
 - ``K`` (the full matrix, built on first access) is the structural CSR: entries that cancel to
   exactly 0.0 are kept, where the reference's LIL storage drops them.
 - Extra keyword ``precision="fp64"|"mixed"|"fp32"`` on solve_static selects the PCG precision

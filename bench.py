@@ -735,7 +735,7 @@ def workload_spmv(args):
         iters[prec] = info.iters
     out = {}
     for prec in ("mixed", "fp64", "fp32"):
-        r = spmv_roofline(op, prec, max(1, args.steps), peak)
+        r = spmv_roofline(op, prec, max(1, args.spmv_reps), peak)
         r["peak_source"] = f"MEASURED_PEAKS.json hbm_gbs (of {kind})"
         out[prec] = r
     return {"metric": "PCG SpMV kernel time, 128x32x32 K_ff (n 418176, nnz 32348142), mixed 48-bit sliced",

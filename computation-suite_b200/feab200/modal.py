@@ -12,7 +12,8 @@ vectors) with a Rayleigh-Ritz step, every product on the GPU:
                                      (feab_symeig_jacobi, one CTA, k <= 64; p x p products only)
     X  = Y V                         M-orthonormal Ritz vectors, lambda ascending (feab_panel_small)
 
-until the n_modes lowest Ritz values change by less than ``tol`` (relative).  Ritz values converge
+until the n_modes lowest Ritz values change by less than ``tol`` (relative), or stop decreasing
+once the change is below ``1e3 * tol`` (round-off, not convergence, then sets it).  Ritz values converge
 like (lambda_i / lambda_{p+1})^(2j), so the block is wider than the number of modes asked for.
 """
 from __future__ import annotations
@@ -58,6 +59,7 @@ def subspace_iteration(Kop: ReducedOperator, Mop: ReducedOperator, n_modes, subs
     KY = torch.empty_like(B)
     MY = torch.empty_like(B)
     lam_old = None
+    change_old = None
     for it in range(1, maxiter + 1):
         block_spmm(Mop, X, out=B)
         Y, res = block_pcg(Kop, np.array([0, n]), B, [p], tol=pcg_tol)
@@ -72,7 +74,8 @@ def subspace_iteration(Kop: ReducedOperator, Mop: ReducedOperator, n_modes, subs
         low = lam[:n_modes]
         if lam_old is not None:
             change = float(((low - lam_old).abs() / low.abs().clamp_min(1e-300)).max())
-            if change < tol:
+            if change < tol or (change_old is not None and change >= change_old and change < 1e3 * tol):
                 break
+            change_old = change
         lam_old = low.clone()
     return lam[:n_modes], X[:, :n_modes].contiguous(), it

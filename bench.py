@@ -17,6 +17,7 @@ rank's time is reported.
 from __future__ import annotations
 
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -190,6 +191,8 @@ def time_steps(prob, precision, tol, steps, warmup, world):
         prob.step(precision, tol)
     torch.cuda.synchronize()
     barrier(world)
+    gc.collect()
+    gc.disable()          # no collector pause of the host inside the timed steps
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n0 = L.lib.feab_launch_count()
     torch.cuda.nvtx.range_push(f"feab_timed_{precision}")     # lets a profiler select the timed steps
@@ -199,6 +202,7 @@ def time_steps(prob, precision, tol, steps, warmup, world):
     end.record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
+    gc.enable()
     launches = int(L.lib.feab_launch_count() - n0)
     ms = start.elapsed_time(end) / steps
     return max_over_ranks(ms, world), x, dc, info, op, launches
@@ -225,11 +229,14 @@ def e2e_steps(c, precision, tol, steps, warmup):
     for _ in range(warmup):
         one()
     torch.cuda.synchronize()
+    gc.collect()
+    gc.disable()
     t0 = time.perf_counter()
     for _ in range(steps):
         U, dc = one()
     torch.cuda.synchronize()
     ms = (time.perf_counter() - t0) * 1e3 / steps
+    gc.enable()
     N, E, n = len(c.mesh.nodes), len(c.mesh.elements), len(c.free)
     h2d = N * 3 * 8 + E * 8 * 4 + n * 8 + 3 * N * 8 + E * 8     # nodes, conn, F_free, U (for dC/drho), rho
     d2h = 3 * N * 8 + E * 8                                      # U, dC/drho

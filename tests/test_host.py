@@ -193,3 +193,49 @@ def test_block_tuning_cache_round_trip(tmp_path):
     open(path, "w").write("{not json")
     assert bt.load_tuning(path) == {}
     assert bt.load_tuning(str(tmp_path / "missing.json")) == {}
+
+
+def test_direct_solve_orderings_on_the_host():
+    """The direct solve's host-side ordering (feab200.direct): on CPU tensors built from the
+    oracle's K_ff, the DOF permutation is a bijection that keeps each node's rows together and in
+    component order, and the ordering along the longest axis gives a band of about one
+    cross-section of nodes (the bandwidth the GPU kernels then size their tiles for)."""
+    import scipy.sparse as sp
+    import torch
+    import oracle as O
+    from feab200.device import Pattern
+    from feab200.direct import coordinate_order, dof_permutation, node_order
+
+    X, el = O.box_mesh(2.0, 0.4, 0.4, 16, 3, 2)
+    fixed = O.fixed_dofs_on_plane(X, 0, 0.0)
+    free = O.free_dofs(3 * len(X), fixed)
+    K = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(X[el], O.D_solid3d(1.0, 0.3)), el, 3 * len(X)),
+                      free).tocsr()
+    node = free // 3
+    starts = np.flatnonzero(np.r_[True, node[1:] != node[:-1]])
+    fm = -np.ones(3 * len(X), np.int32)
+    fm[free] = np.arange(len(free), dtype=np.int32)
+
+    class Op:  # the fields of a ReducedOperator that the ordering reads, on the CPU
+        pattern = Pattern(K.shape[0], K.nnz, len(starts), torch.as_tensor(K.indptr.astype(np.int32)),
+                          torch.as_tensor(K.indices.astype(np.int32)),
+                          torch.as_tensor(np.r_[starts, len(free)].astype(np.int32)), torch.as_tensor(fm))
+        vals64 = torch.as_tensor(K.data)
+        n = K.shape[0]
+
+    op = Op()
+    cross = (3 + 1) * (2 + 1)                        # nodes in one x = const cross-section
+    for order in (node_order(op), coordinate_order(op, X)):
+        assert sorted(order.tolist()) == list(range(len(starts)))
+        iperm = dof_permutation(op, order).numpy()
+        assert sorted(iperm.tolist()) == list(range(op.n))
+        # a node's rows stay consecutive and in component order
+        assert np.all(np.diff(iperm[starts[0]:starts[1]]) == 1)
+        P = sp.csr_matrix((np.ones(op.n), (iperm, np.arange(op.n))), shape=K.shape)
+        Kp = (P @ K @ P.T).tocoo()
+        assert np.allclose(np.sort(np.linalg.eigvalsh(Kp.toarray()))[:3], np.sort(np.linalg.eigvalsh(K.toarray()))[:3])
+    # along the longest axis: within two cross-sections of nodes (3 DOFs each)
+    iperm = dof_permutation(op, coordinate_order(op, X)).numpy()
+    P = sp.csr_matrix((np.ones(op.n), (iperm, np.arange(op.n))), shape=K.shape)
+    Kp = (P @ K @ P.T).tocoo()
+    assert int(np.abs(Kp.row - Kp.col).max()) < 3 * 2 * cross + 3

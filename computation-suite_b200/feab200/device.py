@@ -204,10 +204,18 @@ class DeviceMesh:
         if torch.is_tensor(elements):
             conn = elements.to(device=self.device, dtype=torch.int32).contiguous()
         else:
-            el = np.asarray(elements)
-            if el.size and (el.min() < 0 or el.max() >= coords.shape[0]):
-                raise ValueError("element connectivity refers to node ids outside the mesh")
-            conn = torch.as_tensor(np.ascontiguousarray(el, dtype=np.int32)).to(self.device)
+            # copied as given and range-checked / narrowed to int32 on the device (no host passes)
+            arr = np.ascontiguousarray(elements)
+            if arr.dtype.kind == "u":          # unsigned ids: torch has no general uint64 tensors
+                arr = arr.astype(np.int64)
+            el = torch.as_tensor(arr).to(self.device)
+            if el.dtype.is_floating_point or el.dtype == torch.bool:
+                el = el.to(torch.int64)
+            if el.numel():
+                lo, hi = torch.stack(torch.aminmax(el)).cpu().tolist()   # one read-back
+                if lo < 0 or hi >= coords.shape[0]:
+                    raise ValueError("element connectivity refers to node ids outside the mesh")
+            conn = el.to(torch.int32).contiguous()
         if coords.ndim != 2 or coords.shape[1] != 3:
             raise ValueError(f"hex8 solid mesh needs (n_nodes, 3) coordinates, got {tuple(coords.shape)}")
         if conn.ndim != 2 or conn.shape[1] != 8:

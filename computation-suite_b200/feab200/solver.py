@@ -354,7 +354,8 @@ class FESystem:
         Fv = self.F if F is None else np.asarray(F, dtype=float)
         _, free, fixed, _ = self._bc_arrays()
         u_fixed = self._fixed_dof_values_array(fixed)
-        Ff = torch.as_tensor(np.ascontiguousarray(Fv[free])).to(self.device)
+        # the whole F goes to the device and is gathered there with the cached free-DOF index
+        Ff = torch.as_tensor(np.ascontiguousarray(Fv, dtype=np.float64)).to(self.device)[self._bc_device_index()[0]]
         if fixed.size and np.any(u_fixed):
             v = np.zeros(self.n_dof)
             v[fixed] = u_fixed

@@ -38,7 +38,8 @@ PENAL, RHO_MIN = 3.0, 1e-9
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 20 for the headline workload and the reference arm, 3 otherwise)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--shape", type=int, nargs=3, default=(128, 32, 32))
@@ -54,7 +55,10 @@ def parse():
                     default="cantilever",
                     help="cantilever: the headline (assemble + PCG + dC/drho); the others measure the SIMP "
                          "adjoint, the uneven batch and the snapshot/POD cases")
-    return ap.parse_args()
+    args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 20 if (args.workload == "cantilever" or args.impl == "reference") else 3
+    return args
 
 
 # ----------------------------------------------------------------------------- distributed
@@ -193,19 +197,21 @@ def time_steps(prob, precision, tol, steps, warmup, world):
     barrier(world)
     gc.collect()
     gc.disable()          # no collector pause of the host inside the timed steps
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # an event after every step: the per-step times (no extra synchronisation in the loop)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
     n0 = L.lib.feab_launch_count()
     torch.cuda.nvtx.range_push(f"feab_timed_{precision}")     # lets a profiler select the timed steps
-    start.record()
-    for _ in range(steps):
+    evs[0].record()
+    for i in range(steps):
         x, dc, info, op = prob.step(precision, tol)
-    end.record()
+        evs[i + 1].record()
     torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     gc.enable()
     launches = int(L.lib.feab_launch_count() - n0)
-    ms = start.elapsed_time(end) / steps
-    return max_over_ranks(ms, world), x, dc, info, op, launches
+    ms = evs[0].elapsed_time(evs[-1]) / steps
+    each = [round(evs[i].elapsed_time(evs[i + 1]), 2) for i in range(steps)]
+    return max_over_ranks(ms, world), x, dc, info, op, launches, each
 
 
 def e2e_steps(c, precision, tol, steps, warmup):
@@ -1211,8 +1217,9 @@ def main():
     # plain FP64 first, then mixed (the headline)
     clocks.start()
     clocks.wait_first_sample()
-    ms64, x64, dc64, info64, op64, _ = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
-    ms32, x32, dc32, info32, op, launches = time_steps(prob, "mixed", args.tol, args.steps, args.warmup, world)
+    ms64, x64, dc64, info64, op64, _, each64 = time_steps(prob, "fp64", args.tol, args.steps, args.warmup, world)
+    ms32, x32, dc32, info32, op, launches, each32 = time_steps(prob, "mixed", args.tol, args.steps, args.warmup,
+                                                              world)
     clk = clocks.stop()
     # the FP32-everything variant, one solve, for reference
     t0 = time.perf_counter()
@@ -1270,6 +1277,7 @@ def main():
             "precision": ("mixed: SpMV on 48-bit (36-bit mantissa) values in difference form, FP64 vectors and "
                           "scalars, FP64 reliable residual replacement"),
             "plain_fp64_ms": round(ms64, 3), "mixed_speedup_vs_fp64": round(ms64 / ms32, 3),
+            "step_ms_each": {"mixed": each32, "fp64": each64},
             "fp32_everything_ms": round(msf, 3),
             "iters": {"mixed": info32.iters, "fp64": info64.iters, "fp32": infof.iters,
                       "reliable_updates": info32.reliable_updates},

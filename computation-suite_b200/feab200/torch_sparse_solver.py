@@ -87,10 +87,23 @@ def fesystem_solve_static_torch(sysobj, method="cg", device="cpu", tol=1e-8, max
                 "Kff may not be SPD, or needs a tighter tol/more iterations/a better preconditioner than the "
                 "Jacobi one used here; try method='dense' as a fallback or diagnostic.")
     else:
-        x, info = pcg_solve(op, b, tol=1e-12, maxiter=max_iter, precision="fp64")
-        if info.status in (L.FEAB_NOT_CONVERGED, L.FEAB_NOT_SPD):
-            raise RuntimeError("fesystem_solve_static_torch: method='dense' runs a tight PCG here, and it did not "
-                               "converge (K_ff is not SPD or is singular)")
+        # a direct solve, as the reference's torch_dense_solve: the banded Cholesky of K_ff
+        # (feab200.direct); a K_ff that is not SPD, or singular, goes to a tight PCG instead
+        x = None
+        try:
+            fac = op.direct_factor(coords=getattr(sysobj.mesh, "nodes", None))
+            if not fac.near_singular:
+                x = fac.solve(b)
+        except (MemoryError, np.linalg.LinAlgError):
+            x = None
+        if x is None:
+            x, info = pcg_solve(op, b, tol=1e-12, maxiter=max_iter, precision="fp64")
+            if info.status in (L.FEAB_NOT_CONVERGED, L.FEAB_NOT_SPD):
+                raise RuntimeError("fesystem_solve_static_torch: method='dense' found K_ff not SPD or singular, "
+                                   "and the tight PCG it falls back to did not converge")
+            L.raise_for(info.status, "fesystem_solve_static_torch")
+        U[free] = x.cpu().numpy()
+        return U
     L.raise_for(info.status, "fesystem_solve_static_torch")
     U[free] = x.cpu().numpy()
     return U

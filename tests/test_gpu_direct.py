@@ -129,3 +129,21 @@ def test_band_entry_points_check_their_arguments():
     band = L.Band(0, 0, 0, 0, storage.data_ptr())
     rc = L.lib.feab_band_assemble(C.byref(csr), L.dptr(ident), 0, C.byref(band), L.stream_ptr(dev))
     assert rc == L.FEAB_BAD_ARG
+
+
+def test_torch_backend_dense_method_is_the_direct_solve(golden):
+    """fesystem_solve_static_torch(method="dense") (torch_sparse_solver.py:268-314, a dense LU in
+    the reference) runs the banded Cholesky: the reference's SuperLU solution to 1e-10, and the
+    same answer as the CG method to its tolerance."""
+    import feab200 as feab
+    from feab200.torch_sparse_solver import fesystem_solve_static_torch
+    g = golden("cantilever_20x4x4")
+    mesh = feab.Mesh(nodes=g["nodes"], elements=g["elements"])
+    fs = feab.FESystem(mesh, feab.Hex8Solid3D(), sparse=True)
+    fs.assemble_stiffness(g["D"])
+    fs.fix_dofs(mesh.nodes_on_plane(0, 0.0), [0, 1, 2])
+    fs.add_consistent_facet_load(feab.Hex8Solid3D(), [tuple(f) for f in g["facets"]], 2, -1.0e6)
+    Ud = fesystem_solve_static_torch(fs, method="dense")
+    assert _rel(Ud, g["U_lu"]) < DTOL
+    Uc = fesystem_solve_static_torch(fs, method="cg", tol=1e-10)
+    assert _rel(Uc, Ud) < 1e-8

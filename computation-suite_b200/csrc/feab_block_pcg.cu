@@ -245,27 +245,29 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
       }
     } else {
       // the difference-form operator is packed in 4-column quads (group offsets and lengths are
-      // multiples of 4): one 16-byte column load and, per row, a 16 + 8-byte value load per quad
-      for (int mq = lane; mq < (nc >> 2); mq += 32) {
-        const int m = 4 * mq;
-        const uint4 tq = __ldg(reinterpret_cast<const uint4*>(A.tcol + c0 + cb + m));
-        st.col[m] = (int)tq.x;
-        st.col[m + 1] = (int)tq.y;
-        st.col[m + 2] = (int)tq.z;
-        st.col[m + 3] = (int)tq.w;
-#pragma unroll
-        for (int k = 0; k < 3; ++k) {
-          if (k < f) {
-            const uint4 h = __ldg(reinterpret_cast<const uint4*>(A.vhi + s0 + k * len + cb + m));
-            const uint2 l = __ldg(reinterpret_cast<const uint2*>(A.vlo + s0 + k * len + cb + m));
-            const uint32_t l2 = __ldg(reinterpret_cast<const uint32_t*>(A.vlo2 + s0 + k * len + cb + m));
-            st.val[k][m] = dec56(h.x, l.x, l2);
-            st.val[k][m + 1] = dec56(h.y, l.x >> 16, l2 >> 8);
-            st.val[k][m + 2] = dec56(h.z, l.y, l2 >> 16);
-            st.val[k][m + 3] = dec56(h.w, l.y >> 16, l2 >> 24);
-          } else {
-            st.val[k][m] = st.val[k][m + 1] = st.val[k][m + 2] = st.val[k][m + 3] = 0.0;
-          }
+      // multiples of 4): one 16-byte column load per quad, stored with the tag bits cleared so
+      // the gathers below index with it directly, and a 16 + 8 + 4-byte value load per (row,
+      // quad) pair, the pairs spread over all lanes
+      const int nq = nc >> 2;
+      for (int mq = lane; mq < nq; mq += 32) {
+        const uint4 tq = __ldg(reinterpret_cast<const uint4*>(A.tcol + c0 + cb + 4 * mq));
+        *reinterpret_cast<int4*>(&st.col[4 * mq]) =
+            make_int4((int)(tq.x & 0x3fffffffu), (int)(tq.y & 0x3fffffffu), (int)(tq.z & 0x3fffffffu),
+                      (int)(tq.w & 0x3fffffffu));
+      }
+      for (int pq = lane; pq < 3 * nq; pq += 32) {
+        const int k = pq >= nq ? (pq >= 2 * nq ? 2 : 1) : 0;
+        const int m = 4 * (pq - k * nq);
+        double2* dst = reinterpret_cast<double2*>(&st.val[k][m]);
+        if (k < f) {
+          const int64_t e = s0 + (int64_t)k * len + cb + m;
+          const uint4 h = __ldg(reinterpret_cast<const uint4*>(A.vhi + e));
+          const uint2 l = __ldg(reinterpret_cast<const uint2*>(A.vlo + e));
+          const uint32_t l2 = __ldg(reinterpret_cast<const uint32_t*>(A.vlo2 + e));
+          dst[0] = make_double2(dec56(h.x, l.x, l2), dec56(h.y, l.x >> 16, l2 >> 8));
+          dst[1] = make_double2(dec56(h.z, l.y, l2 >> 16), dec56(h.w, l.y >> 16, l2 >> 24));
+        } else {
+          dst[0] = dst[1] = make_double2(0.0, 0.0);
         }
       }
     }
@@ -287,7 +289,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
 #pragma unroll
         for (int u = 0; u < U; ++u) {
           if (m0 + u < nc) {
-            gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), cl, xv[u]);
+            gather_row<K>(src, (int)t[u], cl, xv[u]);
           } else {
 #pragma unroll
             for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;
@@ -328,7 +330,7 @@ __device__ __forceinline__ void group_spmm(const BArgs& A, int g, int lane, Grou
         const int m = m0 + u * MPW;
         t[u] = m < nc ? (unsigned)st.col[m] : 0u;
         if (m < nc) {
-          gather_row<K>(src, (int)(DIFF ? (t[u] & 0x3fffffffu) : t[u]), cl, xv[u]);
+          gather_row<K>(src, (int)t[u], cl, xv[u]);
         } else {
 #pragma unroll
           for (int q = 0; q < CPL; ++q) xv[u][q] = 0.0;

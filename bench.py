@@ -417,8 +417,9 @@ def _oracle_job(shape, tol, solve_tol, outdir):
 
 class OracleRun:
     """The oracle job of the headline workload, run after the GPU measurements in a separate
-    process: its solution is the FP64 accuracy reference (PCG to 1e-12, SURVEY-style oracle for
-    the large configs) and its phase times are a real full CPU step (not extrapolated)."""
+    process: its solution is the FP64 accuracy reference (the oracle's PCG to 1e-12, which stands
+    in for the reference's sparse direct solve at these sizes) and its phase times are a real full
+    CPU step (not extrapolated)."""
 
     SOLVE_TOL = 1e-12
 

@@ -50,7 +50,7 @@ def _oracle_solve(Kff, b, tol=ORACLE_TOL):
 
 # ----------------------------------------------------------------------------- 128 x 32 x 32
 @pytest.fixture(scope="module")
-def cfg2():
+def cantilever_128x32x32():
     w = W.random_tip_cantilever(128, 32, 32)
     X, el = w["nodes"], w["elements"]
     Kff = O.reduce_free(O.structural_csr(O.hex8_element_stiffness(X[el], w["D"]), el, w["n_dof"]), w["free"])
@@ -59,9 +59,9 @@ def cfg2():
     return w, Kff, x, at
 
 
-def test_cfg2_csr_pattern_and_values_at_size(cfg2):
+def test_csr_pattern_and_values_at_128x32x32(cantilever_128x32x32):
     from feab200.device import DeviceMesh
-    w, Kff, _, _ = cfg2
+    w, Kff, _, _ = cantilever_128x32x32
     dm = DeviceMesh(w["nodes"], w["elements"])
     op = dm.assemble(dm.element_stiffness(w["D"]), dm.pattern(w["fixed"]), want32=False)
     assert (op.n, op.nnz) == (418176, 32348142) == (Kff.shape[0], Kff.nnz)
@@ -77,9 +77,9 @@ def test_cfg2_csr_pattern_and_values_at_size(cfg2):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_cfg2_solution_vs_oracle_at_size(cfg2, precision):
+def test_solution_vs_oracle_at_128x32x32(cantilever_128x32x32, precision):
     from feab200.device import DeviceMesh, pcg_solve
-    w, _, x_ref, at = cfg2
+    w, _, x_ref, at = cantilever_128x32x32
     dm = DeviceMesh(w["nodes"], w["elements"])
     op = dm.assemble(dm.element_stiffness(w["D"]), dm.pattern(w["fixed"]), want32=False)
     x, info = pcg_solve(op, w["F"][w["free"]], tol=BENCH_TOL, precision=precision)
@@ -91,7 +91,7 @@ def test_cfg2_solution_vs_oracle_at_size(cfg2, precision):
 
 # ----------------------------------------------------------------------------- 96 x 32 x 32 SIMP
 @pytest.fixture(scope="module")
-def cfg4():
+def simp_96x32x32():
     w = W.simp_cantilever(96, 32, 32)
     X, el, rho = w["nodes"], w["elements"], w["rho"]
     ke = O.hex8_element_stiffness(X[el], w["D"])
@@ -112,8 +112,8 @@ def _simp_problem(w, precision, tol):
 
 
 @pytest.mark.parametrize("precision", ["fp64", "mixed"])
-def test_cfg4_gradient_vs_closed_form_at_size(cfg4, precision):
-    w, _, _, dc_ref = cfg4
+def test_simp_gradient_vs_closed_form_at_96x32x32(simp_96x32x32, precision):
+    w, _, _, dc_ref = simp_96x32x32
     prob = _simp_problem(w, precision, BENCH_TOL)
     dev = prob.dm.device
     f = torch.as_tensor(w["F"][w["free"]]).to(dev)
@@ -158,8 +158,8 @@ class _Compliance:
         return float(np.dot(self.f, ul) + np.dot(r, ul))
 
 
-def test_cfg4_gradient_vs_central_differences_h1e6(cfg4):
-    w, ke, Kff, dc_ref = cfg4
+def test_simp_gradient_vs_central_differences_h1e6_at_96x32x32(simp_96x32x32):
+    w, ke, Kff, dc_ref = simp_96x32x32
     prob = _simp_problem(w, "mixed", BENCH_TOL)
     dev = prob.dm.device
     f = torch.as_tensor(w["F"][w["free"]]).to(dev)
@@ -183,7 +183,7 @@ def test_cfg4_gradient_vs_central_differences_h1e6(cfg4):
 
 
 # ----------------------------------------------------------------------------- uneven batch
-def test_cfg3_batch_sample_vs_independent_oracle_solves():
+def test_uneven_batch_sample_vs_independent_oracle_solves():
     from feab200 import cantilever
     from feab200.batched import ProblemBatch
     probs = cantilever.batch_cantilevers(256)
@@ -205,7 +205,7 @@ def test_cfg3_batch_sample_vs_independent_oracle_solves():
 
 
 # ----------------------------------------------------------------------------- 192 x 48 x 48
-def test_cfg5_csr_pattern_bit_exact_at_442k_elements():
+def test_csr_pattern_bit_exact_at_192x48x48():
     from feab200.device import DeviceMesh
     nodes, el = O.box_mesh(2.0, 0.4, 0.4, 192, 48, 48)
     fixed = O.fixed_dofs_on_plane(nodes)

@@ -39,7 +39,7 @@ def _reduced(nodes, elements, D, fixed, want32=True):
 
 
 # ----------------------------------------------------------------------------- pattern + values
-def test_csr_pattern_bit_exact_and_values_cfg1(golden):
+def test_csr_pattern_bit_exact_and_values_20x4x4(golden):
     g = golden("cantilever_20x4x4")
     dm, op = _reduced(g["nodes"], g["elements"], g["D"], g["fixed"])
     p = op.pattern

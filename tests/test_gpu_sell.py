@@ -33,7 +33,7 @@ def _check(op, Kff, xs):
         assert np.linalg.norm(ymx - ref) / scale < 1e-10
 
 
-def test_sell_spmv_matches_csr_cfg1(golden):
+def test_sell_spmv_matches_csr_20x4x4(golden):
     g = golden("cantilever_20x4x4")
     op = _reduced(g["nodes"], g["elements"], g["D"], g["fixed"])
     Kff = sp.csr_matrix((g["vals"], g["col_idx"], g["row_ptr"]))

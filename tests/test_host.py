@@ -18,7 +18,7 @@ def test_box_mesh_matches_oracle(shape):
     assert np.array_equal(m.nodes, nodes) and np.array_equal(m.elements, el)
 
 
-def test_config1_inputs_match_reference(golden):
+def test_cantilever_20x4x4_inputs_match_reference(golden):
     g = golden("cantilever_20x4x4")
     c = cl.plain_cantilever()
     assert np.array_equal(c.mesh.nodes, g["nodes"])
